@@ -1,0 +1,235 @@
+// Shared helpers of the sm_100a PF-FLIP library: error state, launch
+// accounting, storage-type conversion, index helpers and deterministic block
+// reductions.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <cstdio>
+
+#include "pfflip.h"
+
+namespace pf {
+
+// ---------------------------------------------------------------- errors
+void set_error(int code, const char* fmt, ...);
+void set_cuda_error(cudaError_t e, const char* where);
+void count_launch(uint64_t n = 1);
+
+#define PF_REQUIRE(cond, ...)                    \
+  do {                                           \
+    if (!(cond)) {                               \
+      ::pf::set_error(PF_ERR_ARG, __VA_ARGS__);  \
+      return PF_ERR_ARG;                         \
+    }                                            \
+  } while (0)
+
+#define PF_CUDA_TRY(expr)                                   \
+  do {                                                      \
+    cudaError_t e_ = (expr);                                \
+    if (e_ != cudaSuccess) {                                \
+      ::pf::set_cuda_error(e_, #expr);                      \
+      return PF_ERR_CUDA;                                   \
+    }                                                       \
+  } while (0)
+
+// after a kernel launch
+#define PF_LAUNCHED()                                       \
+  do {                                                      \
+    cudaError_t e_ = cudaGetLastError();                    \
+    if (e_ != cudaSuccess) {                                \
+      ::pf::set_cuda_error(e_, "kernel launch");            \
+      return PF_ERR_CUDA;                                   \
+    }                                                       \
+    ::pf::count_launch();                                   \
+  } while (0)
+
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+constexpr int kNumSMs = 148;
+
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// ---------------------------------------------------------------- storage types
+template <class T> struct Store;
+template <> struct Store<float> {
+  static __device__ __forceinline__ float ld(const float* p) { return *p; }
+  static __device__ __forceinline__ void st(float* p, float v) { *p = v; }
+};
+template <> struct Store<__half> {
+  static __device__ __forceinline__ float ld(const __half* p) { return __half2float(*p); }
+  static __device__ __forceinline__ void st(__half* p, float v) { *p = __float2half_rn(v); }
+};
+template <> struct Store<__nv_bfloat16> {
+  static __device__ __forceinline__ float ld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+  static __device__ __forceinline__ void st(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+};
+
+template <class T> __device__ __forceinline__ float ldT(const T* p) { return Store<T>::ld(p); }
+// the value a float becomes when stored as T and read back
+template <class T> __device__ __forceinline__ float roundT(float v) {
+  T t;
+  Store<T>::st(&t, v);
+  return Store<T>::ld(&t);
+}
+template <class T> __device__ __forceinline__ void stT(T* p, float v) { Store<T>::st(p, v); }
+
+// ---------------------------------------------------------------- index helpers
+struct Dim3i {
+  int n0, n1, n2;
+  __host__ __device__ __forceinline__ long long at(int i, int j, int k) const {
+    return ((long long)i * n1 + j) * n2 + k;
+  }
+  __host__ __device__ __forceinline__ long long size() const { return (long long)n0 * n1 * n2; }
+};
+
+__host__ __device__ __forceinline__ Dim3i face_dims(int nx, int ny, int nz, int axis) {
+  return Dim3i{nx + (axis == 0), ny + (axis == 1), nz + (axis == 2)};
+}
+
+// ---------------------------------------------------------------- reductions
+// Block-wide sum of a double; result valid in thread 0.  blockDim.x must be a
+// multiple of 32 and <= 1024.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+template <int NT> __device__ __forceinline__ double block_sum(double v, double* sh /*>= 32*/) {
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (w == 0) {
+    r = (l < NT / 32) ? sh[l] : 0.0;
+    r = warp_sum(r);
+  }
+  __syncthreads();
+  return r;
+}
+
+template <int NT> __device__ __forceinline__ float block_max(float v, float* sh /*>= 32*/) {
+  v = warp_max(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  float r = 0.f;
+  if (w == 0) {
+    r = (l < NT / 32) ? sh[l] : 0.f;
+    r = warp_max(r);
+  }
+  __syncthreads();
+  return r;
+}
+
+// Deterministic grid reduction: every block writes its partial, the last
+// block to arrive (ticket on *counter) sums the partials in block order with a
+// fixed tree and resets the counter.  Returns true in the last block (all
+// threads), with *result valid in every thread of that block.
+template <int NT>
+__device__ __forceinline__ bool grid_sum_last(double partial_in_t0, double* partials, unsigned* counter,
+                                              double* result, double* sh) {
+  __shared__ bool s_last;
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = partial_in_t0;
+    __threadfence();
+    unsigned t = atomicAdd(counter, 1u);
+    s_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+  double v = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += NT) v += ((volatile double*)partials)[b];
+  v = block_sum<NT>(v, sh);
+  if (threadIdx.x == 0) {
+    sh[32] = v;
+    *counter = 0u;
+  }
+  __syncthreads();
+  *result = sh[32];
+  return true;
+}
+
+// Two sums at once (same protocol; partials holds 2*gridDim.x doubles).
+template <int NT>
+__device__ __forceinline__ bool grid_sum2_last(double a_t0, double b_t0, double* partials, unsigned* counter,
+                                               double* ra, double* rb, double* sh) {
+  __shared__ bool s_last;
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = a_t0;
+    partials[2 * blockIdx.x + 1] = b_t0;
+    __threadfence();
+    unsigned t = atomicAdd(counter, 1u);
+    s_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+  double va = 0.0, vb = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += NT) {
+    va += ((volatile double*)partials)[2 * b];
+    vb += ((volatile double*)partials)[2 * b + 1];
+  }
+  va = block_sum<NT>(va, sh);
+  vb = block_sum<NT>(vb, sh);
+  if (threadIdx.x == 0) {
+    sh[32] = va;
+    sh[33] = vb;
+    *counter = 0u;
+  }
+  __syncthreads();
+  *ra = sh[32];
+  *rb = sh[33];
+  return true;
+}
+
+template <int NT>
+__device__ __forceinline__ bool grid_max_last(float partial_in_t0, double* partials, unsigned* counter,
+                                              float* result, float* shf) {
+  __shared__ bool s_last;
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = (double)partial_in_t0;
+    __threadfence();
+    unsigned t = atomicAdd(counter, 1u);
+    s_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+  float v = 0.f;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += NT) v = fmaxf(v, (float)((volatile double*)partials)[b]);
+  v = block_max<NT>(v, shf);
+  if (threadIdx.x == 0) {
+    shf[32] = v;
+    *counter = 0u;
+  }
+  __syncthreads();
+  *result = shf[32];
+  return true;
+}
+
+// float max via integer atomics (valid for non-negative floats)
+__device__ __forceinline__ void atomic_max_nonneg(float* addr, float v) {
+  atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));
+}
+
+inline int grid_for(long long n, int nt, int max_blocks) {
+  long long b = (n + nt - 1) / nt;
+  if (b < 1) b = 1;
+  if (b > max_blocks) b = max_blocks;
+  return (int)b;
+}
+
+}  // namespace pf

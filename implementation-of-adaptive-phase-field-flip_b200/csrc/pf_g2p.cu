@@ -1,0 +1,196 @@
+// Grid-to-particle transfer and advection in one particle pass on sm_100a.
+//
+// The reference runs field_difference x3 (pfflip/kernels.py:499-502), g2p
+// (:468-496), the liquid extrapolation, advect_rk3 (:508-549) and
+// reflect_at_walls (:567-595) as separate launches (pfflip/sim.py:316-341,
+// :408-420).  The extrapolation only reads grid fields, so it runs first and
+// a single kernel then does, per particle, the FLIP/PIC update, the Ralston
+// RK3 trace through the extrapolated (liquid) or raw (air) field, the clamp
+// and the wall reflection.  u - u* is formed per interpolation tap, which is
+// the reference's interpolation of the difference field, value for value.
+// Particles are in cell order, so neighbouring threads gather neighbouring
+// taps from L1/L2.
+#include "pf_common.cuh"
+
+namespace pf {
+
+struct G2PArgs {
+  long long n;
+  int nx, ny, nz;
+  float dx, dt, a_liq, a_air;
+  float lo[3], hi[3];
+  float4* pos;
+  float4* vel;
+  const float* u[3];
+  const float* us[3];
+  const float* ul[3];
+  const int* solid;
+  int do_g2p, do_advect;
+};
+
+// clamped trilinear sample of face grid `c` (pfflip/kernels.py:52-79); q = x/dx.
+// DIFF: samples f - fs tap by tap.
+template <bool DIFF>
+__device__ __forceinline__ float sample_face(const float* __restrict__ f, const float* __restrict__ fs, int c,
+                                             const float q[3], int nx, int ny, int nz) {
+  const int n0 = nx + (c == 0), n1 = ny + (c == 1), n2 = nz + (c == 2);
+  const float g0 = q[0] - (c == 0 ? 0.f : 0.5f);
+  const float g1 = q[1] - (c == 1 ? 0.f : 0.5f);
+  const float g2 = q[2] - (c == 2 ? 0.f : 0.5f);
+  const int i0 = (int)floorf(g0), j0 = (int)floorf(g1), k0 = (int)floorf(g2);
+  const float tx = g0 - (float)i0, ty = g1 - (float)j0, tz = g2 - (float)k0;
+  float acc = 0.f;
+#pragma unroll
+  for (int di = 0; di < 2; ++di) {
+    const float wi = di == 0 ? 1.f - tx : tx;
+    const int ii = min(max(i0 + di, 0), n0 - 1);
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj) {
+      const float wj = dj == 0 ? 1.f - ty : ty;
+      const int jj = min(max(j0 + dj, 0), n1 - 1);
+      const long long row = ((long long)ii * n1 + jj) * n2;
+#pragma unroll
+      for (int dk = 0; dk < 2; ++dk) {
+        const float wk = dk == 0 ? 1.f - tz : tz;
+        const int kk = min(max(k0 + dk, 0), n2 - 1);
+        float v = __ldg(f + row + kk);
+        if (DIFF) v = v - __ldg(fs + row + kk);
+        acc += wi * wj * wk * v;
+      }
+    }
+  }
+  return acc;
+}
+
+__device__ __forceinline__ void sample_vel(const float* const f[3], const float x[3], float dx, int nx, int ny, int nz,
+                                           float out[3]) {
+  const float q[3] = {x[0] / dx, x[1] / dx, x[2] / dx};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) out[c] = sample_face<false>(f[c], nullptr, c, q, nx, ny, nz);
+}
+
+__global__ void __launch_bounds__(256) k_g2p_advect(G2PArgs a) {
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
+    float4 P = a.pos[p];
+    float4 V = a.vel[p];
+    const int flags = __float_as_int(P.w);
+    const int pstate = (flags >> PF_PSTATE_SHIFT) & 3;
+    const bool liquid = (flags & PF_FLAG_LIQUID) != 0;
+    float x[3] = {P.x, P.y, P.z};
+    float v[3] = {V.x, V.y, V.z};
+    if (a.do_g2p && pstate == 0) {
+      const float alpha = liquid ? a.a_liq : a.a_air;
+      const float q[3] = {x[0] / a.dx, x[1] / a.dx, x[2] / a.dx};
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float delta = sample_face<true>(a.u[c], a.us[c], c, q, a.nx, a.ny, a.nz);
+        const float pic = sample_face<false>(a.u[c], nullptr, c, q, a.nx, a.ny, a.nz);
+        v[c] = alpha * (v[c] + delta) + (1.f - alpha) * pic;
+      }
+    }
+    if (a.do_advect) {
+      if (pstate == 0) {
+        const float* const* f = liquid ? a.ul : a.u;
+        float k1[3], k2[3], k3[3], y[3];
+        sample_vel(f, x, a.dx, a.nx, a.ny, a.nz, k1);
+        const float h1 = 0.5f * a.dt, h2 = 0.75f * a.dt;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) y[c] = x[c] + h1 * k1[c];
+        sample_vel(f, y, a.dx, a.nx, a.ny, a.nz, k2);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) y[c] = x[c] + h2 * k2[c];
+        sample_vel(f, y, a.dx, a.nx, a.ny, a.nz, k3);
+        const float c1 = 2.0f / 9.0f, c2 = 3.0f / 9.0f, c3 = 4.0f / 9.0f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float xn = x[c] + a.dt * (c1 * k1[c] + c2 * k2[c] + c3 * k3[c]);
+          x[c] = fminf(fmaxf(xn, a.lo[c]), a.hi[c]);
+        }
+      }
+      if (pstate != 2) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (x[c] <= a.lo[c]) {
+            x[c] = a.lo[c];
+            v[c] = fmaxf(v[c], 0.f);
+          } else if (x[c] >= a.hi[c]) {
+            x[c] = a.hi[c];
+            v[c] = fminf(v[c], 0.f);
+          }
+        }
+        if (a.solid) {  // pfflip/kernels.py:630-679
+          const int nx = a.nx, ny = a.ny, nz = a.nz;
+          const int i = min(max((int)(x[0] / a.dx), 0), nx - 1);
+          const int j = min(max((int)(x[1] / a.dx), 0), ny - 1);
+          const int k = min(max((int)(x[2] / a.dx), 0), nz - 1);
+          if (a.solid[((long long)i * ny + j) * nz + k] != 0) {
+            float best = 1.0e9f;
+            int bax = 0, bsg = 1;
+            for (int d = 0; d < 6; ++d) {
+              const int ax = d / 2, sg = (d % 2 == 0) ? -1 : 1;
+              for (int t = 1; t < 8; ++t) {
+                const int ii = i + (ax == 0 ? sg * t : 0), jj = j + (ax == 1 ? sg * t : 0),
+                          kk = k + (ax == 2 ? sg * t : 0);
+                if (ii < 0 || jj < 0 || kk < 0 || ii >= nx || jj >= ny || kk >= nz) break;
+                if (a.solid[((long long)ii * ny + jj) * nz + kk] == 0) {
+                  const float dist = (float)t;
+                  if (dist < best) {
+                    best = dist;
+                    bax = ax;
+                    bsg = sg;
+                  }
+                  break;
+                }
+              }
+            }
+            if (best <= 1.0e8f) {
+              const float off = (best + 0.5f) * a.dx * (float)bsg;
+              x[bax] = x[bax] + off;
+              if ((float)bsg * v[bax] < 0.f) v[bax] = 0.f;
+            }
+          }
+        }
+      }
+    }
+    P.x = x[0]; P.y = x[1]; P.z = x[2];
+    V.x = v[0]; V.y = v[1]; V.z = v[2];
+    a.pos[p] = P;
+    a.vel[p] = V;
+  }
+}
+
+}  // namespace pf
+
+using namespace pf;
+
+extern "C" int pf_g2p_advect(const pf_grid* g, int64_t n, float* pos4, float* vel4, const float* vel_x,
+                             const float* vel_y, const float* vel_z, const float* vstar_x, const float* vstar_y,
+                             const float* vstar_z, const float* vliq_x, const float* vliq_y, const float* vliq_z,
+                             const int32_t* solid, float alpha_liquid, float alpha_air, float dt, const float lo[3],
+                             const float hi[3], int32_t do_g2p, int32_t do_advect, void* stream) {
+  PF_REQUIRE(g && pos4 && vel4 && vel_x && vel_y && vel_z, "null argument");
+  PF_REQUIRE(!do_g2p || (vstar_x && vstar_y && vstar_z), "u* fields required for G2P");
+  PF_REQUIRE(!do_advect || (vliq_x && vliq_y && vliq_z && lo && hi), "extrapolated fields and bounds required");
+  PF_REQUIRE(aligned16(pos4) && aligned16(vel4), "particle streams must be 16-byte aligned");
+  if (n <= 0) return PF_OK;
+  G2PArgs a;
+  a.n = n;
+  a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
+  a.dx = g->dx; a.dt = dt;
+  a.a_liq = alpha_liquid; a.a_air = alpha_air;
+  for (int c = 0; c < 3; ++c) {
+    a.lo[c] = lo ? lo[c] : 0.f;
+    a.hi[c] = hi ? hi[c] : 0.f;
+  }
+  a.pos = reinterpret_cast<float4*>(pos4);
+  a.vel = reinterpret_cast<float4*>(vel4);
+  a.u[0] = vel_x; a.u[1] = vel_y; a.u[2] = vel_z;
+  a.us[0] = vstar_x; a.us[1] = vstar_y; a.us[2] = vstar_z;
+  a.ul[0] = vliq_x; a.ul[1] = vliq_y; a.ul[2] = vliq_z;
+  a.solid = solid;
+  a.do_g2p = do_g2p;
+  a.do_advect = do_advect;
+  k_g2p_advect<<<grid_for(n, 256, kNumSMs * 16), 256, 0, S(stream)>>>(a);
+  PF_LAUNCHED();
+  return PF_OK;
+}

@@ -1,0 +1,450 @@
+// Grid-side streaming stages of the PF-FLIP step on sm_100a: face velocities,
+// eq. (7) phase field and eq. (9) coefficients with the wall/solid zeroing
+// fused into one pass; forces; divergence right-hand side; projection; the
+// divergence norm; liquid velocity extrapolation (all sweeps of one face array
+// in one shared-memory pass); CFL speed.
+#include "pf_common.cuh"
+
+namespace pf {
+
+// eq. (7), pfflip/kernels.py:234-241
+__device__ __forceinline__ float phase_field(float rho, float rho_min, float alpha_phi, float rho_0l) {
+  if (rho < rho_min) return 0.f;
+  return fminf(sqrtf(fmaxf(rho - rho_min, 0.f) / (alpha_phi * rho_0l)), 1.f);
+}
+
+struct FaceSpace {  // the three face arrays and the cells as one index space
+  int nx, ny, nz;
+  long long nf[3], nc;
+  __device__ __forceinline__ long long total() const { return nf[0] + nf[1] + nf[2] + nc; }
+};
+
+__host__ __device__ inline FaceSpace make_space(int nx, int ny, int nz) {
+  FaceSpace s;
+  s.nx = nx; s.ny = ny; s.nz = nz;
+  s.nf[0] = (long long)(nx + 1) * ny * nz;
+  s.nf[1] = (long long)nx * (ny + 1) * nz;
+  s.nf[2] = (long long)nx * ny * (nz + 1);
+  s.nc = (long long)nx * ny * nz;
+  return s;
+}
+
+// splits a flat index into (axis, face index, i, j, k); axis 3 = cell
+__device__ __forceinline__ int locate(const FaceSpace& s, long long e, long long* f, int* i, int* j, int* k) {
+  int a = 0;
+  while (a < 3 && e >= s.nf[a]) { e -= s.nf[a]; ++a; }
+  const int n1 = s.ny + (a == 1), n2 = s.nz + (a == 2);
+  *f = e;
+  *k = (int)(e % n2);
+  const long long t = e / n2;
+  *j = (int)(t % n1);
+  *i = (int)(t / n1);
+  return a;
+}
+
+__device__ __forceinline__ bool boundary_face(int a, int i, int j, int k, int nx, int ny, int nz) {
+  const int n = a == 0 ? i : a == 1 ? j : k;
+  const int last = a == 0 ? nx : a == 1 ? ny : nz;
+  return n == 0 || n == last;
+}
+
+__device__ __forceinline__ bool solid_face(const int* solid, int a, int i, int j, int k, int nx, int ny, int nz) {
+  if (!solid) return false;
+  const int im = i - (a == 0), jm = j - (a == 1), km = k - (a == 2);
+  bool b = false;
+  if (i < nx && j < ny && k < nz) b = b || solid[((long long)i * ny + j) * nz + k] != 0;
+  if (im >= 0 && jm >= 0 && km >= 0) b = b || solid[((long long)im * ny + jm) * nz + km] != 0;
+  return b;
+}
+
+struct PhaseArgs {
+  FaceSpace s;
+  const float* mass[3];
+  const float* mom[3];
+  const float* cmass;
+  const int* solid;
+  float eps, rho_min, alpha_phi, rho_0l, rho_l, rho_g;
+  float* vel[3];
+  int* valid[3];
+  float* phi_cell;
+  int* is_liq;
+  float* phi_face[3];
+  float* beta[3];
+};
+
+__global__ void k_phase_beta(PhaseArgs a) {
+  const FaceSpace& S = a.s;
+  const int nx = S.nx, ny = S.ny, nz = S.nz;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < S.total();
+       e += (long long)gridDim.x * blockDim.x) {
+    long long f;
+    int i, j, k;
+    const int ax = locate(S, e, &f, &i, &j, &k);
+    if (ax == 3) {  // cell: pfflip/kernels.py:244-255
+      const float phi = phase_field(a.cmass[f], a.rho_min, a.alpha_phi, a.rho_0l);
+      a.phi_cell[f] = phi;
+      a.is_liq[f] = phi >= 0.5f ? 1 : 0;
+      continue;
+    }
+    // face velocity, pfflip/kernels.py:212-228
+    const float m = a.mass[ax][f];
+    const bool ok = m > a.eps;
+    float u = ok ? a.mom[ax][f] / m : 0.f;
+    if (a.valid[ax]) a.valid[ax][f] = ok ? 1 : 0;
+    // face phase field and beta, pfflip/kernels.py:258-311
+    const int im = i - (ax == 0), jm = j - (ax == 1), km = k - (ax == 2);
+    const bool lo_out = im < 0 || jm < 0 || km < 0;
+    const bool hi_out = i >= nx || j >= ny || k >= nz;
+    int A = 0, B = 0;
+    if (!lo_out)
+      A = phase_field(a.cmass[((long long)im * ny + jm) * nz + km], a.rho_min, a.alpha_phi, a.rho_0l) >= 0.5f;
+    if (!hi_out) B = phase_field(a.cmass[((long long)i * ny + j) * nz + k], a.rho_min, a.alpha_phi, a.rho_0l) >= 0.5f;
+    if (lo_out) A = B;
+    if (hi_out) B = A;
+    float phi;
+    if (A == 1 && B == 1) phi = 1.f;
+    else if (A == 0 && B == 0) phi = 0.f;
+    else phi = phase_field(m, a.rho_min, a.alpha_phi, a.rho_0l);
+    if (a.phi_face[ax]) a.phi_face[ax][f] = phi;
+    float beta = 1.f / ((1.f - phi) * a.rho_g + phi * a.rho_l);
+    // walls and obstacles, pfflip/kernels.py:314-326 and :601-627
+    if (boundary_face(ax, i, j, k, nx, ny, nz) || solid_face(a.solid, ax, i, j, k, nx, ny, nz)) {
+      beta = 0.f;
+      u = 0.f;
+    }
+    a.beta[ax][f] = beta;
+    a.vel[ax][f] = u;
+  }
+}
+
+struct ForceArgs {
+  FaceSpace s;
+  float* vel[3];
+  float* vstar[3];
+  const int* solid;
+  float g[3];
+  float dt;
+};
+
+// vel_star = vel; vel += g*dt; walls/obstacles zeroed (pfflip/sim.py:176-177, :270-285)
+__global__ void k_save_force(ForceArgs a) {
+  const FaceSpace& S = a.s;
+  const long long nfaces = S.nf[0] + S.nf[1] + S.nf[2];
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nfaces;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long f;
+    int i, j, k;
+    const int ax = locate(S, e, &f, &i, &j, &k);
+    float v = a.vel[ax][f];
+    if (a.vstar[ax]) a.vstar[ax][f] = v;
+    if (a.g[ax] != 0.f) v += a.g[ax] * a.dt;
+    if (boundary_face(ax, i, j, k, S.nx, S.ny, S.nz) || solid_face(a.solid, ax, i, j, k, S.nx, S.ny, S.nz)) v = 0.f;
+    a.vel[ax][f] = v;
+  }
+}
+
+__device__ __forceinline__ float divergence(const float* u, const float* v, const float* w, int i, int j, int k,
+                                            int nx, int ny, int nz) {
+  const long long fu = ((long long)i * ny + j) * nz + k;
+  const long long fv = ((long long)i * (ny + 1) + j) * nz + k;
+  const long long fw = ((long long)i * ny + j) * (nz + 1) + k;
+  return (u[fu + (long long)ny * nz] - u[fu]) + (v[fv + nz] - v[fv]) + (w[fw + 1] - w[fw]);
+}
+
+// pfflip/kernels.py:338-363
+__global__ void k_build_rhs(int nx, int ny, int nz, const float* __restrict__ u, const float* __restrict__ v,
+                            const float* __restrict__ w, const float* __restrict__ wsum, float* __restrict__ b,
+                            float dx, float dt, float rho_0, float k_div) {
+  const long long n = (long long)nx * ny * nz;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(c % nz);
+    const long long t = c / nz;
+    const int j = (int)(t % ny), i = (int)(t / ny);
+    const float du = divergence(u, v, w, i, j, k, nx, ny, nz);
+    float rhs = -(dx / dt) * du;
+    if (k_div > 0.f) {
+      const float excess = (wsum[c] - rho_0) / rho_0;
+      rhs -= dx * dx * k_div * fmaxf(excess, 0.f) / dt;
+    }
+    b[c] = rhs;
+  }
+}
+
+struct ProjArgs {
+  FaceSpace s;
+  const float* p;
+  const float* beta[3];
+  float* vel[3];
+  float dx, dt;
+};
+
+// pfflip/kernels.py:366-387
+__global__ void k_project(ProjArgs a) {
+  const FaceSpace& S = a.s;
+  const long long nfaces = S.nf[0] + S.nf[1] + S.nf[2];
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nfaces;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long f;
+    int i, j, k;
+    const int ax = locate(S, e, &f, &i, &j, &k);
+    const float bc = a.beta[ax][f];
+    if (bc == 0.f) continue;
+    const int im = i - (ax == 0), jm = j - (ax == 1), km = k - (ax == 2);
+    if (im < 0 || jm < 0 || km < 0) continue;
+    if (i >= S.nx || j >= S.ny || k >= S.nz) continue;
+    const float pi = a.p[((long long)i * S.ny + j) * S.nz + k];
+    const float pm = a.p[((long long)im * S.ny + jm) * S.nz + km];
+    a.vel[ax][f] -= a.dt * bc * (pi - pm) / a.dx;
+  }
+}
+
+// max |div u|/dx (pfflip/kernels.py:390-400)
+__global__ void __launch_bounds__(256) k_max_div(int nx, int ny, int nz, const float* __restrict__ u,
+                                                 const float* __restrict__ v, const float* __restrict__ w, float dx,
+                                                 float* out) {
+  __shared__ float sh[40];
+  const long long n = (long long)nx * ny * nz;
+  float m = 0.f;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(c % nz);
+    const long long t = c / nz;
+    const int j = (int)(t % ny), i = (int)(t / ny);
+    const float d = divergence(u, v, w, i, j, k, nx, ny, nz);
+    const float q = fabsf(d / dx);
+    m = fmaxf(m, isnan(q) ? INFINITY : q);
+  }
+  m = block_max<256>(m, sh);
+  if (threadIdx.x == 0) atomic_max_nonneg(out, m);
+}
+
+// ---------------------------------------------------------------- extrapolation
+// One face array (axis ax) per launch.  A CTA owns EX_TI x EX_TJ x EX_TK faces,
+// loads them with an H-face halo (H = sweeps), seeds (pfflip/kernels.py:406-425)
+// and runs H Jacobi sweeps (pfflip/kernels.py:428-462) in shared memory, then
+// writes its tile.  Entries outside the face array are marked absent: they are
+// never updated and never counted, as the reference skips out-of-range
+// neighbours.  Errors from the missing outer halo travel one entry per sweep
+// and never reach the tile.
+constexpr int EX_TI = 4, EX_TJ = 8, EX_TK = 32, EX_NT = 256;
+enum : unsigned char { EX_UNKNOWN = 0, EX_KNOWN = 1, EX_ABSENT = 2 };
+
+__global__ void __launch_bounds__(EX_NT) k_extrapolate(int nx, int ny, int nz, int ax, int H,
+                                                       const float* __restrict__ vel, const int* __restrict__ is_liq,
+                                                       float* __restrict__ vel_liq, int* __restrict__ known_out) {
+  extern __shared__ __align__(16) unsigned char exsm[];
+  const int n0 = nx + (ax == 0), n1 = ny + (ax == 1), n2 = nz + (ax == 2);
+  const int R0 = EX_TI + 2 * H, R1 = EX_TJ + 2 * H, R2 = EX_TK + 2 * H;
+  const int RN = R0 * R1 * R2;
+  float* V0 = reinterpret_cast<float*>(exsm);
+  float* V1 = V0 + RN;
+  unsigned char* K0 = reinterpret_cast<unsigned char*>(V1 + RN);
+  unsigned char* K1 = K0 + RN;
+  const int i0 = blockIdx.z * EX_TI - H, j0 = blockIdx.y * EX_TJ - H, k0 = blockIdx.x * EX_TK - H;
+  for (int e = threadIdx.x; e < RN; e += EX_NT) {
+    const int r2 = e % R2, t = e / R2, r1 = t % R1, r0 = t / R1;
+    const int i = i0 + r0, j = j0 + r1, k = k0 + r2;
+    if (i < 0 || j < 0 || k < 0 || i >= n0 || j >= n1 || k >= n2) {
+      V0[e] = 0.f;
+      K0[e] = EX_ABSENT;
+      continue;
+    }
+    const int im = i - (ax == 0), jm = j - (ax == 1), km = k - (ax == 2);
+    int liq = 0;
+    if (i < nx && j < ny && k < nz) liq = max(liq, is_liq[((long long)i * ny + j) * nz + k]);
+    if (im >= 0 && jm >= 0 && km >= 0) liq = max(liq, is_liq[((long long)im * ny + jm) * nz + km]);
+    V0[e] = (liq == 1) ? vel[((long long)i * n1 + j) * n2 + k] : 0.f;
+    K0[e] = (liq == 1) ? EX_KNOWN : EX_UNKNOWN;
+  }
+  __syncthreads();
+  float *Vi = V0, *Vo = V1;
+  unsigned char *Ki = K0, *Ko = K1;
+  const int st[3] = {R1 * R2, R2, 1};
+  for (int s = 0; s < H; ++s) {
+    for (int e = threadIdx.x; e < RN; e += EX_NT) {
+      const unsigned char kn = Ki[e];
+      if (kn != EX_UNKNOWN) {
+        Vo[e] = Vi[e];
+        Ko[e] = kn;
+        continue;
+      }
+      const int r2 = e % R2, t = e / R2, r1 = t % R1, r0 = t / R1;
+      const int rr[3] = {r0, r1, r2}, RR[3] = {R0, R1, R2};
+      float acc = 0.f;
+      int cnt = 0;
+#pragma unroll
+      for (int d = 0; d < 6; ++d) {
+        const int a = d >> 1, sg = (d & 1) ? 1 : -1;
+        const int q = rr[a] + sg;
+        if (q < 0 || q >= RR[a]) continue;
+        const int nb = e + sg * st[a];
+        if (Ki[nb] == EX_KNOWN) {
+          acc += Vi[nb];
+          cnt += 1;
+        }
+      }
+      if (cnt > 0) {
+        Vo[e] = acc / (float)cnt;
+        Ko[e] = EX_KNOWN;
+      } else {
+        Vo[e] = Vi[e];
+        Ko[e] = EX_UNKNOWN;
+      }
+    }
+    __syncthreads();
+    float* tv = Vi; Vi = Vo; Vo = tv;
+    unsigned char* tk = Ki; Ki = Ko; Ko = tk;
+  }
+  for (int e = threadIdx.x; e < EX_TI * EX_TJ * EX_TK; e += EX_NT) {
+    const int c2 = e % EX_TK, t = e / EX_TK, c1 = t % EX_TJ, c0 = t / EX_TJ;
+    const int i = i0 + H + c0, j = j0 + H + c1, k = k0 + H + c2;
+    if (i >= n0 || j >= n1 || k >= n2) continue;
+    const int r = ((c0 + H) * R1 + (c1 + H)) * R2 + (c2 + H);
+    const long long g = ((long long)i * n1 + j) * n2 + k;
+    vel_liq[g] = Vi[r];
+    if (known_out) known_out[g] = (Ki[r] == EX_KNOWN) ? 1 : 0;
+  }
+}
+
+// CFL speed over particles with pstate == 0 (pfflip/kernels.py:552-564)
+__global__ void __launch_bounds__(256) k_max_speed(long long n, const float4* __restrict__ pos,
+                                                   const float4* __restrict__ vel, float* out) {
+  __shared__ float sh[40];
+  float m = 0.f;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    const int flags = __float_as_int(__ldg(&pos[p].w));
+    if ((flags >> PF_PSTATE_SHIFT) & 3) continue;
+    const float4 v = __ldg(vel + p);
+    m = fmaxf(m, sqrtf(v.x * v.x + v.y * v.y + v.z * v.z));
+  }
+  m = block_max<256>(m, sh);
+  if (threadIdx.x == 0) atomic_max_nonneg(out, m);
+}
+
+int ew_blocks(long long n) { return grid_for(n, 256, kNumSMs * 16); }
+
+}  // namespace pf
+
+using namespace pf;
+
+extern "C" {
+
+int pf_phase_beta(const pf_grid* g, const float* mass_x, const float* mass_y, const float* mass_z,
+                  const float* mom_x, const float* mom_y, const float* mom_z, const float* cell_mass,
+                  const int32_t* solid, float mass_eps, float rho_min, float alpha_phi, float rho_0l, float rho_l,
+                  float rho_g, float* vel_x, float* vel_y, float* vel_z, int32_t* valid_x, int32_t* valid_y,
+                  int32_t* valid_z, float* phi_cell, int32_t* is_liquid, float* phi_face_x, float* phi_face_y,
+                  float* phi_face_z, float* beta_x, float* beta_y, float* beta_z, void* stream) {
+  PF_REQUIRE(g && mass_x && mass_y && mass_z && mom_x && mom_y && mom_z && cell_mass && vel_x && vel_y && vel_z &&
+                 phi_cell && is_liquid && beta_x && beta_y && beta_z,
+             "null argument");
+  PhaseArgs a;
+  a.s = make_space(g->nx, g->ny, g->nz);
+  a.mass[0] = mass_x; a.mass[1] = mass_y; a.mass[2] = mass_z;
+  a.mom[0] = mom_x; a.mom[1] = mom_y; a.mom[2] = mom_z;
+  a.cmass = cell_mass;
+  a.solid = solid;
+  a.eps = mass_eps; a.rho_min = rho_min; a.alpha_phi = alpha_phi; a.rho_0l = rho_0l;
+  a.rho_l = rho_l; a.rho_g = rho_g;
+  a.vel[0] = vel_x; a.vel[1] = vel_y; a.vel[2] = vel_z;
+  a.valid[0] = valid_x; a.valid[1] = valid_y; a.valid[2] = valid_z;
+  a.phi_cell = phi_cell; a.is_liq = is_liquid;
+  a.phi_face[0] = phi_face_x; a.phi_face[1] = phi_face_y; a.phi_face[2] = phi_face_z;
+  a.beta[0] = beta_x; a.beta[1] = beta_y; a.beta[2] = beta_z;
+  const long long tot = a.s.nf[0] + a.s.nf[1] + a.s.nf[2] + a.s.nc;
+  k_phase_beta<<<ew_blocks(tot), 256, 0, S(stream)>>>(a);
+  PF_LAUNCHED();
+  return PF_OK;
+}
+
+int pf_save_and_force(const pf_grid* g, float* vel_x, float* vel_y, float* vel_z, float* vel_star_x,
+                      float* vel_star_y, float* vel_star_z, const int32_t* solid, float gx, float gy, float gz,
+                      float dt, void* stream) {
+  PF_REQUIRE(g && vel_x && vel_y && vel_z, "null argument");
+  ForceArgs a;
+  a.s = make_space(g->nx, g->ny, g->nz);
+  a.vel[0] = vel_x; a.vel[1] = vel_y; a.vel[2] = vel_z;
+  a.vstar[0] = vel_star_x; a.vstar[1] = vel_star_y; a.vstar[2] = vel_star_z;
+  a.solid = solid;
+  a.g[0] = gx; a.g[1] = gy; a.g[2] = gz;
+  a.dt = dt;
+  k_save_force<<<ew_blocks(a.s.nf[0] + a.s.nf[1] + a.s.nf[2]), 256, 0, S(stream)>>>(a);
+  PF_LAUNCHED();
+  return PF_OK;
+}
+
+int pf_build_rhs(const pf_grid* g, const float* vel_x, const float* vel_y, const float* vel_z,
+                 const float* cell_wsum, float* b, float dt, float rho_0, float k_div, void* stream) {
+  PF_REQUIRE(g && vel_x && vel_y && vel_z && b, "null argument");
+  PF_REQUIRE(k_div <= 0.f || cell_wsum, "cell_wsum required when k_div > 0");
+  const long long n = (long long)g->nx * g->ny * g->nz;
+  k_build_rhs<<<ew_blocks(n), 256, 0, S(stream)>>>(g->nx, g->ny, g->nz, vel_x, vel_y, vel_z, cell_wsum, b, g->dx, dt,
+                                                   rho_0, k_div);
+  PF_LAUNCHED();
+  return PF_OK;
+}
+
+int pf_project(const pf_grid* g, const float* p, const float* beta_x, const float* beta_y, const float* beta_z,
+               float* vel_x, float* vel_y, float* vel_z, float dt, void* stream) {
+  PF_REQUIRE(g && p && beta_x && beta_y && beta_z && vel_x && vel_y && vel_z, "null argument");
+  ProjArgs a;
+  a.s = make_space(g->nx, g->ny, g->nz);
+  a.p = p;
+  a.beta[0] = beta_x; a.beta[1] = beta_y; a.beta[2] = beta_z;
+  a.vel[0] = vel_x; a.vel[1] = vel_y; a.vel[2] = vel_z;
+  a.dx = g->dx;
+  a.dt = dt;
+  k_project<<<ew_blocks(a.s.nf[0] + a.s.nf[1] + a.s.nf[2]), 256, 0, S(stream)>>>(a);
+  PF_LAUNCHED();
+  return PF_OK;
+}
+
+int pf_max_divergence(const pf_grid* g, const float* vel_x, const float* vel_y, const float* vel_z, float* out,
+                      void* stream) {
+  PF_REQUIRE(g && vel_x && vel_y && vel_z && out, "null argument");
+  cudaStream_t s = S(stream);
+  PF_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float), s));
+  const long long n = (long long)g->nx * g->ny * g->nz;
+  k_max_div<<<ew_blocks(n), 256, 0, s>>>(g->nx, g->ny, g->nz, vel_x, vel_y, vel_z, g->dx, out);
+  PF_LAUNCHED();
+  return PF_OK;
+}
+
+int pf_extrapolate(const pf_grid* g, const float* vel_x, const float* vel_y, const float* vel_z,
+                   const int32_t* is_liquid, int32_t sweeps, float* vel_liq_x, float* vel_liq_y, float* vel_liq_z,
+                   int32_t* known_x, int32_t* known_y, int32_t* known_z, void* stream) {
+  PF_REQUIRE(g && vel_x && vel_y && vel_z && is_liquid && vel_liq_x && vel_liq_y && vel_liq_z, "null argument");
+  PF_REQUIRE(sweeps >= 0 && sweeps <= 4, "sweeps must be in [0, 4]");
+  const float* vin[3] = {vel_x, vel_y, vel_z};
+  float* vout[3] = {vel_liq_x, vel_liq_y, vel_liq_z};
+  int* kout[3] = {known_x, known_y, known_z};
+  const int H = sweeps;
+  const size_t rn = (size_t)(EX_TI + 2 * H) * (EX_TJ + 2 * H) * (EX_TK + 2 * H);
+  const size_t smem = rn * (2 * sizeof(float) + 2);
+  static int attr_done = 0;
+  if (!attr_done) {
+    PF_CUDA_TRY(cudaFuncSetAttribute(k_extrapolate, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    attr_done = 1;
+  }
+  for (int ax = 0; ax < 3; ++ax) {
+    const int n0 = g->nx + (ax == 0), n1 = g->ny + (ax == 1), n2 = g->nz + (ax == 2);
+    dim3 grid((n2 + EX_TK - 1) / EX_TK, (n1 + EX_TJ - 1) / EX_TJ, (n0 + EX_TI - 1) / EX_TI);
+    k_extrapolate<<<grid, EX_NT, smem, S(stream)>>>(g->nx, g->ny, g->nz, ax, H, vin[ax], is_liquid, vout[ax],
+                                                    kout[ax]);
+    PF_LAUNCHED();
+  }
+  return PF_OK;
+}
+
+int pf_particle_max_speed(int64_t n, const float* pos4, const float* vel4, float* out, void* stream) {
+  PF_REQUIRE(n >= 0 && pos4 && vel4 && out, "null argument");
+  PF_REQUIRE(aligned16(pos4) && aligned16(vel4), "particle streams must be 16-byte aligned");
+  cudaStream_t s = S(stream);
+  PF_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float), s));
+  if (n == 0) return PF_OK;
+  k_max_speed<<<ew_blocks(n), 256, 0, s>>>(n, reinterpret_cast<const float4*>(pos4),
+                                           reinterpret_cast<const float4*>(vel4), out);
+  PF_LAUNCHED();
+  return PF_OK;
+}
+
+}  // extern "C"

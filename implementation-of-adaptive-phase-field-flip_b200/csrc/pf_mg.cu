@@ -1,0 +1,1295 @@
+// Variable-coefficient Poisson solver for sm_100a: aggregation Galerkin
+// multigrid (red-black weighted Gauss-Seidel smoother) preconditioning a
+// Polak-Ribiere flexible CG.  Follows the algorithm of pfflip/poisson.py
+// (apply_A :54-88, rbgs_sweep :105-126, galerkin_coarsen_faces :130-163,
+// restrict_sum :166-175, prolong_inject_add :178-182, MGPCG :240-409) with a
+// B200-first kernel structure:
+//
+// * one kernel per red+black sweep.  A CTA owns a (j,k) tile of 8x32 cells and
+//   an i-range, marches along i with a 4-plane ring of p (2-cell halo) in
+//   shared memory, updates colour 1 on plane m (tile + 1-cell ring), then
+//   colour 2 on plane m-1 (tile), and writes plane m-1 — colour 2 lags colour
+//   1 by one plane.  Input and output p are different buffers (ping-pong), so
+//   halos never mix old and new values across CTAs.  The result equals the
+//   reference's two half-sweep launches.
+// * the residual is fused with restriction, the prolongation with the first
+//   post-smoothing sweep, a zero initial guess skips the p read, and the mean
+//   of the level-0 V-cycle output is reduced inside the last sweep.
+// * CG scalars never leave the device: every reduction is a deterministic
+//   two-level FP64 sum (block partials, then the last CTA sums them in block
+//   order), and the last CTA also forms alpha/beta and the stop test.  Every
+//   kernel reads a device "done" flag, so the host can enqueue (or replay as a
+//   CUDA graph) one CG iteration ahead and poll convergence one iteration late
+//   without changing the result.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "pf_common.cuh"
+
+namespace pf {
+
+// --------------------------------------------------------------- device state
+struct MGState {
+  double rz, qAq, alpha, beta, bnorm, rel, rz_new, rpz;
+  double sum_last;
+  float c_shift;   // float(-mean) of the last mean reduction
+  float alpha_f, neg_alpha_f, beta_f;
+  float tol;
+  float scale_r;   // 16-bit storage: level-0 b = r * scale_r
+  float zscale;    // 16-bit storage: z = p_lp * zscale
+  float maxabs_last;
+  int32_t it, done, status, max_iter;
+};
+static_assert(sizeof(MGState) <= PF_MG_STATE_BYTES, "state size");
+
+enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_BREAKDOWN = 2, ST_NONFINITE = 3, ST_ZERO_RHS = 4 };
+
+// counters used by the last-CTA reductions (one per call site so that two
+// reductions in flight never share a ticket)
+enum {
+  CNT_SUM_B = 0, CNT_INIT_R, CNT_INIT_Q, CNT_APPLY_DOT, CNT_UPDATE_XR, CNT_DOTS, CNT_SWEEP_MEAN, CNT_FINAL_SUM,
+  CNT_COARSE, CNT_PRECOND, CNT_SCALE, CNT_MAX
+};
+static_assert(CNT_MAX <= PF_MG_COUNTERS, "counters");
+
+constexpr int RED_NT = 256;
+constexpr int RED_MAX_BLOCKS = 2 * kNumSMs * 4;  // 1184 partials per reduction
+constexpr int64_t kPartials = RED_MAX_BLOCKS * 2 * 4;
+
+__device__ __forceinline__ bool is_done(const MGState* st) { return st != nullptr && st->done != 0; }
+
+// --------------------------------------------------------------- apply_A
+// pfflip/poisson.py:54-75 with clamped neighbour indices and diag formed on
+// the fly in compute_diag's order (pfflip/poisson.py:49-51) when diag is null.
+__device__ __forceinline__ float apply_row(const float* __restrict__ p, const float* __restrict__ bx,
+                                           const float* __restrict__ by, const float* __restrict__ bz,
+                                           const float* __restrict__ diag, int nx, int ny, int nz, int i, int j,
+                                           int k, int flux) {
+  const long long c = ((long long)i * ny + j) * nz + k;
+  const long long fxi = c;                                  // bx(i,j,k) = (i*ny + j)*nz + k
+  const long long fxu = c + (long long)ny * nz;             // bx(i+1,j,k)
+  const long long fyi = ((long long)i * (ny + 1) + j) * nz + k;
+  const long long fyu = fyi + nz;
+  const long long fzi = ((long long)i * ny + j) * (nz + 1) + k;
+  const long long fzu = fzi + 1;
+  const float bxl = bx[fxi], bxu = bx[fxu], byl = by[fyi], byu = by[fyu], bzl = bz[fzi], bzu = bz[fzu];
+  const long long sI = (long long)ny * nz;
+  const float pc = p[c];
+  const float p0 = p[i > 0 ? c - sI : c], p1 = p[i < nx - 1 ? c + sI : c];
+  const float p2 = p[j > 0 ? c - nz : c], p3 = p[j < ny - 1 ? c + nz : c];
+  const float p4 = p[k > 0 ? c - 1 : c], p5 = p[k < nz - 1 ? c + 1 : c];
+  if (flux) {
+    float s = bxl * (pc - p0);
+    s += bxu * (pc - p1);
+    s += byl * (pc - p2);
+    s += byu * (pc - p3);
+    s += bzl * (pc - p4);
+    s += bzu * (pc - p5);
+    return s;
+  }
+  const float d = diag ? diag[c] : (bxl + bxu + byl + byu + bzl + bzu);
+  float s = bxl * p0;
+  s += bxu * p1;
+  s += byl * p2;
+  s += byu * p3;
+  s += bzl * p4;
+  s += bzu * p5;
+  return d * pc - s;
+}
+
+__global__ void k_apply_A(int nx, int ny, int nz, const float* __restrict__ p, const float* __restrict__ bx,
+                          const float* __restrict__ by, const float* __restrict__ bz, const float* __restrict__ diag,
+                          float* __restrict__ out, int flux) {
+  const long long n = (long long)nx * ny * nz;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(c % nz);
+    const long long t = c / nz;
+    const int j = (int)(t % ny), i = (int)(t / ny);
+    out[c] = apply_row(p, bx, by, bz, diag, nx, ny, nz, i, j, k, flux);
+  }
+}
+
+// --------------------------------------------------------------- hierarchy build
+template <class T>
+__global__ void k_level_coefs(int nx, int ny, int nz, const float* __restrict__ bx, const float* __restrict__ by,
+                              const float* __restrict__ bz, float* __restrict__ diag, T* bx_lp, T* by_lp, T* bz_lp,
+                              float lp_scale) {
+  // diag (pfflip/poisson.py:41-51) and, in 16-bit mode, the scaled copies
+  const long long nc = (long long)nx * ny * nz;
+  const long long nfx = (long long)(nx + 1) * ny * nz, nfy = (long long)nx * (ny + 1) * nz,
+                  nfz = (long long)nx * ny * (nz + 1);
+  const long long tot = nc + (bx_lp ? nfx + nfy + nfz : 0);
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    if (e < nc) {
+      const int k = (int)(e % nz);
+      const long long t = e / nz;
+      const int j = (int)(t % ny), i = (int)(t / ny);
+      const long long fyi = ((long long)i * (ny + 1) + j) * nz + k;
+      const long long fzi = ((long long)i * ny + j) * (nz + 1) + k;
+      diag[e] = bx[e] + bx[e + (long long)ny * nz] + by[fyi] + by[fyi + nz] + bz[fzi] + bz[fzi + 1];
+    } else {
+      long long f = e - nc;
+      if (f < nfx) stT(bx_lp + f, bx[f] * lp_scale);
+      else if ((f -= nfx) < nfy) stT(by_lp + f, by[f] * lp_scale);
+      else { f -= nfy; stT(bz_lp + f, bz[f] * lp_scale); }
+    }
+  }
+}
+
+// pfflip/poisson.py:130-163 for all three axes in one launch
+__global__ void k_coarsen_faces(int fx, int fy, int fz, int cx, int cy, int cz, const float* __restrict__ fbx,
+                                const float* __restrict__ fby, const float* __restrict__ fbz, float* __restrict__ cbx,
+                                float* __restrict__ cby, float* __restrict__ cbz) {
+  const long long ncx = (long long)(cx + 1) * cy * cz, ncy = (long long)cx * (cy + 1) * cz,
+                  ncz = (long long)cx * cy * (cz + 1);
+  const long long tot = ncx + ncy + ncz;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    int axis;
+    long long f = e;
+    Dim3i cd, fd;
+    const float* fine;
+    float* coarse;
+    if (f < ncx) { axis = 0; cd = face_dims(cx, cy, cz, 0); fd = face_dims(fx, fy, fz, 0); fine = fbx; coarse = cbx; }
+    else if ((f -= ncx) < ncy) { axis = 1; cd = face_dims(cx, cy, cz, 1); fd = face_dims(fx, fy, fz, 1); fine = fby; coarse = cby; }
+    else { f -= ncy; axis = 2; cd = face_dims(cx, cy, cz, 2); fd = face_dims(fx, fy, fz, 2); fine = fbz; coarse = cbz; }
+    const int K = (int)(f % cd.n2);
+    const long long t = f / cd.n2;
+    const int J = (int)(t % cd.n1), I = (int)(t / cd.n1);
+    const int i0 = 2 * I, j0 = 2 * J, k0 = 2 * K;
+    float acc = 0.f;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        int ii, jj, kk;
+        if (axis == 0) { ii = i0; jj = j0 + a; kk = k0 + b; }
+        else if (axis == 1) { ii = i0 + a; jj = j0; kk = k0 + b; }
+        else { ii = i0 + a; jj = j0 + b; kk = k0; }
+        if (ii < fd.n0 && jj < fd.n1 && kk < fd.n2) acc += fine[fd.at(ii, jj, kk)];
+      }
+    coarse[f] = acc;
+  }
+}
+
+// --------------------------------------------------------------- fused red-black sweep
+constexpr int SW_TJ = 8, SW_TK = 32, SW_NT = SW_TJ * SW_TK;
+constexpr int SW_PJ = SW_TJ + 4, SW_PK = SW_TK + 4;  // p plane with 2-cell ring
+constexpr int SW_CJ = SW_TJ + 2, SW_CK = SW_TK + 2;  // coefficient plane with 1-cell ring
+
+template <class T, class TB> struct SweepArgs {
+  int n0, n1, n2;
+  int ci;                  // planes per CTA along i
+  const T* p_in;           // ignored when zero_in
+  T* p_out;
+  const TB* b;
+  const float* b_scale;    // device scalar (may be null = 1)
+  const T* bx;
+  const T* by;
+  const T* bz;
+  const T* pc;             // prolongation source (coarse p) or null
+  float pc_scale;
+  float omega;
+  int first_color;
+  int zero_in;
+  double* partials;        // mean accumulation of p_out (null = off)
+  unsigned* counter;
+  MGState* st;             // done flag + mean output (may be null)
+  int n_total;             // cells of the level (mean divisor)
+  int mixed;               // mean is of p*zscale (16-bit hierarchy)
+  int flux;                // PF_STENCIL_FLUX rows
+};
+
+__device__ __forceinline__ int mod3(int m) { return ((m % 3) + 3) % 3; }
+
+template <class T, class TB>
+__global__ void __launch_bounds__(SW_NT) k_rb_sweep(SweepArgs<T, TB> a) {
+  if (is_done(a.st)) return;
+  __shared__ float sP[4][SW_PJ][SW_PK];
+  __shared__ float sB[2][SW_CJ][SW_CK];
+  __shared__ float sBY[2][SW_CJ + 1][SW_CK];
+  __shared__ float sBZ[2][SW_CJ][SW_CK + 1];
+  __shared__ float sBX[3][SW_CJ][SW_CK];
+  __shared__ double sred[40];
+
+  const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
+  const int k0 = blockIdx.x * SW_TK, j0 = blockIdx.y * SW_TJ;
+  const int ia = blockIdx.z * a.ci, ib = min(n0, ia + a.ci);
+  const int tid = threadIdx.x;
+  const long long sI = (long long)n1 * n2;
+  const float bsc = a.b_scale ? *a.b_scale : 1.f;
+  const int c1 = a.first_color, c2 = a.first_color ^ 1;
+  const int hn1 = n1 >> 1, hn2 = n2 >> 1;
+
+  auto load_p_plane = [&](int i) {
+    float(*P)[SW_PK] = sP[i & 3];
+    for (int e = tid; e < SW_PJ * SW_PK; e += SW_NT) {
+      const int r = e / SW_PK, c = e % SW_PK;
+      const int j = j0 - 2 + r, k = k0 - 2 + c;
+      float v = 0.f;
+      if (i >= 0 && i < n0 && j >= 0 && j < n1 && k >= 0 && k < n2) {
+        const long long g = i * sI + (long long)j * n2 + k;
+        if (!a.zero_in) v = ldT(a.p_in + g);
+        if (a.pc) v += ldT(a.pc + ((long long)(i >> 1) * hn1 + (j >> 1)) * hn2 + (k >> 1)) * a.pc_scale;
+      }
+      P[r][c] = v;
+    }
+  };
+  auto load_cell_coefs = [&](int i) {  // b, by, bz of cell plane i
+    const int s = i & 1;
+    const bool iin = (i >= 0 && i < n0);
+    for (int e = tid; e < SW_CJ * SW_CK; e += SW_NT) {
+      const int r = e / SW_CK, c = e % SW_CK;
+      const int j = j0 - 1 + r, k = k0 - 1 + c;
+      const bool in = iin && j >= 0 && j < n1 && k >= 0 && k < n2;
+      sB[s][r][c] = in ? ldT(a.b + i * sI + (long long)j * n2 + k) * bsc : 0.f;
+    }
+    for (int e = tid; e < (SW_CJ + 1) * SW_CK; e += SW_NT) {
+      const int r = e / SW_CK, c = e % SW_CK;
+      const int j = j0 - 1 + r, k = k0 - 1 + c;
+      const bool in = iin && j >= 0 && j <= n1 && k >= 0 && k < n2;
+      sBY[s][r][c] = in ? ldT(a.by + ((long long)i * (n1 + 1) + j) * n2 + k) : 0.f;
+    }
+    for (int e = tid; e < SW_CJ * (SW_CK + 1); e += SW_NT) {
+      const int r = e / (SW_CK + 1), c = e % (SW_CK + 1);
+      const int j = j0 - 1 + r, k = k0 - 1 + c;
+      const bool in = iin && j >= 0 && j < n1 && k >= 0 && k <= n2;
+      sBZ[s][r][c] = in ? ldT(a.bz + ((long long)i * n1 + j) * (n2 + 1) + k) : 0.f;
+    }
+  };
+  auto load_bx_plane = [&](int f) {  // x-faces of plane f (between cells f-1 and f)
+    float(*X)[SW_CK] = sBX[mod3(f)];
+    const bool fin = (f >= 0 && f <= n0);
+    for (int e = tid; e < SW_CJ * SW_CK; e += SW_NT) {
+      const int r = e / SW_CK, c = e % SW_CK;
+      const int j = j0 - 1 + r, k = k0 - 1 + c;
+      const bool in = fin && j >= 0 && j < n1 && k >= 0 && k < n2;
+      X[r][c] = in ? ldT(a.bx + (long long)f * sI + (long long)j * n2 + k) : 0.f;
+    }
+  };
+  // one Gauss-Seidel update of cell (m, r-1, c-1) of the coefficient frame
+  auto relax = [&](int m, int r, int c) {
+    float(*Pm)[SW_PK] = sP[m & 3];
+    const float(*Pl)[SW_PK] = sP[(m - 1) & 3];
+    const float(*Pu)[SW_PK] = sP[(m + 1) & 3];
+    const int s = m & 1;
+    const float bxl = sBX[mod3(m)][r][c], bxu = sBX[mod3(m + 1)][r][c];
+    const float byl = sBY[s][r][c], byu = sBY[s][r + 1][c];
+    const float bzl = sBZ[s][r][c], bzu = sBZ[s][r][c + 1];
+    const float d = bxl + bxu + byl + byu + bzl + bzu;
+    if (!(d > 0.f)) return;
+    const int pr = r + 1, pc = c + 1;
+    const float pv = Pm[pr][pc];
+    float res;
+    if (a.flux) {
+      float sum = bxl * (pv - Pl[pr][pc]);
+      sum += bxu * (pv - Pu[pr][pc]);
+      sum += byl * (pv - Pm[pr - 1][pc]);
+      sum += byu * (pv - Pm[pr + 1][pc]);
+      sum += bzl * (pv - Pm[pr][pc - 1]);
+      sum += bzu * (pv - Pm[pr][pc + 1]);
+      res = sB[s][r][c] - sum;
+    } else {
+      float sum = bxl * Pl[pr][pc];
+      sum += bxu * Pu[pr][pc];
+      sum += byl * Pm[pr - 1][pc];
+      sum += byu * Pm[pr + 1][pc];
+      sum += bzl * Pm[pr][pc - 1];
+      sum += bzu * Pm[pr][pc + 1];
+      res = sB[s][r][c] - (d * pv - sum);
+    }
+    Pm[pr][pc] = pv + a.omega * res / d;
+  };
+
+  // prologue: p planes ia-2, ia-1 and x-face plane ia-1
+  load_p_plane(ia - 2);
+  load_p_plane(ia - 1);
+  load_bx_plane(ia - 1);
+  double msum = 0.0;
+  const int ty = tid / SW_TK, tx = tid % SW_TK;
+
+  for (int m = ia - 1; m <= ib; ++m) {
+    load_p_plane(m + 1);
+    load_cell_coefs(m);
+    load_bx_plane(m + 1);
+    __syncthreads();
+    // colour 1 on plane m over the tile and its 1-cell ring
+    if (m >= 0 && m < n0) {
+      for (int e = tid; e < SW_CJ * SW_CK; e += SW_NT) {
+        const int r = e / SW_CK, c = e % SW_CK;
+        const int j = j0 - 1 + r, k = k0 - 1 + c;
+        if (j < 0 || j >= n1 || k < 0 || k >= n2) continue;
+        if (((m + j + k) & 1) != c1) continue;
+        relax(m, r, c);
+      }
+    }
+    __syncthreads();
+    // colour 2 on plane m-1 over the tile, then write the plane
+    const int mb = m - 1;
+    if (mb >= ia && mb < ib) {
+      const int j = j0 + ty, k = k0 + tx;
+      if (j < n1 && k < n2) {
+        if (((mb + j + k) & 1) == c2) relax(mb, ty + 1, tx + 1);
+        const float v = sP[mb & 3][ty + 2][tx + 2];
+        stT(a.p_out + mb * sI + (long long)j * n2 + k, v);
+        if (a.partials) msum += (double)roundT<T>(v);
+      }
+    }
+    __syncthreads();
+  }
+
+  if (a.partials) {
+    const double bs = block_sum<SW_NT>(msum, sred);
+    const int nb = gridDim.x * gridDim.y * gridDim.z;
+    const int bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    __shared__ bool s_last;
+    if (tid == 0) {
+      a.partials[bid] = bs;
+      __threadfence();
+      s_last = (atomicAdd(a.counter, 1u) == (unsigned)nb - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      double v = 0.0;
+      for (int q = tid; q < nb; q += SW_NT) v += ((volatile double*)a.partials)[q];
+      v = block_sum<SW_NT>(v, sred);
+      if (tid == 0) {
+        a.st->sum_last = v;
+        a.st->c_shift = (float)(-(v / (double)a.n_total) * (a.mixed ? (double)a.st->zscale : 1.0));
+        *a.counter = 0u;
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------------- residual + restriction
+// coarse b = rscale * sum over the 8 fine cells of (b - A p)  (pfflip/poisson.py:91-102, :166-175)
+template <class T, class TB>
+__global__ void k_residual_restrict(int n0, int n1, int n2, const T* __restrict__ p, const TB* __restrict__ b,
+                                    const float* b_scale, const T* __restrict__ bx, const T* __restrict__ by,
+                                    const T* __restrict__ bz, T* __restrict__ cb, float rscale, float* fine_r,
+                                    const MGState* st, int flux) {
+  if (is_done(st)) return;
+  const int C0 = n0 >> 1, C1 = n1 >> 1, C2 = n2 >> 1;
+  const long long nc = (long long)C0 * C1 * C2;
+  const float bsc = b_scale ? *b_scale : 1.f;
+  const long long sI = (long long)n1 * n2;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nc; e += (long long)gridDim.x * blockDim.x) {
+    const int K = (int)(e % C2);
+    const long long t = e / C2;
+    const int J = (int)(t % C1), I = (int)(t / C1);
+    float acc = 0.f;
+#pragma unroll
+    for (int aa = 0; aa < 2; ++aa)
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+          const int i = 2 * I + aa, j = 2 * J + bb, k = 2 * K + cc;
+          const long long c = i * sI + (long long)j * n2 + k;
+          const long long fyi = ((long long)i * (n1 + 1) + j) * n2 + k;
+          const long long fzi = ((long long)i * n1 + j) * (n2 + 1) + k;
+          const float bxl = ldT(bx + c), bxu = ldT(bx + c + sI), byl = ldT(by + fyi), byu = ldT(by + fyi + n2),
+                      bzl = ldT(bz + fzi), bzu = ldT(bz + fzi + 1);
+          const float pv = ldT(p + c);
+          const float q0 = ldT(p + (i > 0 ? c - sI : c)), q1 = ldT(p + (i < n0 - 1 ? c + sI : c));
+          const float q2 = ldT(p + (j > 0 ? c - n2 : c)), q3 = ldT(p + (j < n1 - 1 ? c + n2 : c));
+          const float q4 = ldT(p + (k > 0 ? c - 1 : c)), q5 = ldT(p + (k < n2 - 1 ? c + 1 : c));
+          float Ap;
+          if (flux) {
+            float s = bxl * (pv - q0);
+            s += bxu * (pv - q1);
+            s += byl * (pv - q2);
+            s += byu * (pv - q3);
+            s += bzl * (pv - q4);
+            s += bzu * (pv - q5);
+            Ap = s;
+          } else {
+            const float d = bxl + bxu + byl + byu + bzl + bzu;
+            float s = bxl * q0;
+            s += bxu * q1;
+            s += byl * q2;
+            s += byu * q3;
+            s += bzl * q4;
+            s += bzu * q5;
+            Ap = d * pv - s;
+          }
+          const float r = ldT(b + c) * bsc - Ap;
+          if (fine_r) fine_r[c] = r;
+          acc += r;
+        }
+    stT(cb + e, acc * rscale);
+  }
+}
+
+// --------------------------------------------------------------- coarsest level
+// The coarsest level runs `coarsest` red-black sweeps from p = 0 followed by
+// mean removal (pfflip/poisson.py:325-328) in one CTA with the level in shared
+// memory (levels up to kCoarseMaxCells cells; larger ones use the sweep
+// kernel).  Arithmetic in AccT: float reproduces the reference, double is the
+// FP64 coarsest solve of the 16-bit hierarchy.  Kernel: k_coarsest_b below.
+constexpr int kCoarseMaxCells = 4096;
+constexpr int CO_NT = 512;
+
+// --------------------------------------------------------------- CG vector kernels
+// Sum of b (for the mean); last CTA stores c_shift = float(-sum/n).
+__global__ void __launch_bounds__(RED_NT) k_sum_mean(long long n, const float* __restrict__ x, double* partials,
+                                                     unsigned* counter, MGState* st) {
+  __shared__ double sh[40];
+  double s = 0.0;
+  for (long long e = blockIdx.x * (long long)RED_NT + threadIdx.x; e < n; e += (long long)gridDim.x * RED_NT)
+    s += (double)x[e];
+  s = block_sum<RED_NT>(s, sh);
+  double tot;
+  if (grid_sum_last<RED_NT>(s, partials, counter, &tot, sh) && threadIdx.x == 0) {
+    st->sum_last = tot;
+    st->c_shift = (float)(-(tot / (double)n));
+  }
+}
+
+// r = rhs = b + c_shift; x = 0; bnorm = max|r|; stop if bnorm == 0
+// (pfflip/poisson.py:363-372)
+__global__ void __launch_bounds__(RED_NT) k_init_r(long long n, const float* __restrict__ b, float* __restrict__ rhs,
+                                                   float* __restrict__ r, float* __restrict__ x, double* partials,
+                                                   unsigned* counter, MGState* st) {
+  __shared__ float shf[40];
+  const float c = st->c_shift;
+  float m = 0.f;
+  for (long long e = blockIdx.x * (long long)RED_NT + threadIdx.x; e < n; e += (long long)gridDim.x * RED_NT) {
+    const float v = b[e] + c;
+    if (rhs) rhs[e] = v;
+    r[e] = v;
+    x[e] = 0.f;
+    m = fmaxf(m, isfinite(v) ? fabsf(v) : INFINITY);
+  }
+  m = block_max<RED_NT>(m, shf);
+  float tot;
+  if (grid_max_last<RED_NT>(m, partials, counter, &tot, shf) && threadIdx.x == 0) {
+    st->bnorm = (double)tot;
+    st->rel = 1.0;
+    st->it = 0;
+    st->status = ST_RUNNING;
+    st->done = 0;
+    if (!(tot > 0.f) || isinf(tot)) {
+      st->done = 1;
+      st->status = (tot == 0.f) ? ST_ZERO_RHS : ST_NONFINITE;
+      st->rel = (tot == 0.f) ? 0.0 : 1.0;
+    }
+    // 16-bit hierarchy: b of level 0 is r * scale_r, a power of two putting max|r| in [0.5, 1)
+    int ex = 0;
+    frexpf(tot > 0.f ? tot : 1.f, &ex);
+    st->scale_r = ldexpf(1.f, -ex);
+  }
+}
+
+// z = p*zscale + c_shift, the preconditioned residual (pfflip/poisson.py:351-352)
+template <class T>
+__device__ __forceinline__ float zval(const T* p, long long e, float zs, float c) {
+  return ldT(p + e) * zs + c;
+}
+
+// q = z; rz = <r, z>   (pfflip/poisson.py:378-380)
+template <class T>
+__global__ void __launch_bounds__(RED_NT) k_init_q(long long n, const T* __restrict__ p, const float* __restrict__ r,
+                                                   float* __restrict__ q, float* __restrict__ zout, double* partials,
+                                                   unsigned* counter, MGState* st, int mixed) {
+  if (is_done(st)) return;
+  __shared__ double sh[40];
+  const float c = st->c_shift, zs = mixed ? st->zscale : 1.f;
+  double s = 0.0;
+  for (long long e = blockIdx.x * (long long)RED_NT + threadIdx.x; e < n; e += (long long)gridDim.x * RED_NT) {
+    const float z = zval(p, e, zs, c);
+    q[e] = z;
+    if (zout) zout[e] = z;
+    s += (double)r[e] * (double)z;
+  }
+  s = block_sum<RED_NT>(s, sh);
+  double tot;
+  if (grid_sum_last<RED_NT>(s, partials, counter, &tot, sh) && threadIdx.x == 0) st->rz = tot;
+}
+
+// Ap = A q; qAq = <q, Ap>; it += 1; alpha = rz/qAq or stop when qAq <= 0
+// (pfflip/poisson.py:384-389)
+__global__ void __launch_bounds__(RED_NT) k_apply_dot(int nx, int ny, int nz, const float* __restrict__ q,
+                                                      const float* __restrict__ bx, const float* __restrict__ by,
+                                                      const float* __restrict__ bz, const float* __restrict__ diag,
+                                                      float* __restrict__ Ap, double* partials, unsigned* counter,
+                                                      MGState* st, int flux) {
+  if (is_done(st)) return;
+  __shared__ double sh[40];
+  const long long n = (long long)nx * ny * nz;
+  double s = 0.0;
+  for (long long c = blockIdx.x * (long long)RED_NT + threadIdx.x; c < n; c += (long long)gridDim.x * RED_NT) {
+    const int k = (int)(c % nz);
+    const long long t = c / nz;
+    const int j = (int)(t % ny), i = (int)(t / ny);
+    const float v = apply_row(q, bx, by, bz, diag, nx, ny, nz, i, j, k, flux);
+    Ap[c] = v;
+    s += (double)q[c] * (double)v;
+  }
+  s = block_sum<RED_NT>(s, sh);
+  double tot;
+  if (grid_sum_last<RED_NT>(s, partials, counter, &tot, sh) && threadIdx.x == 0) {
+    st->it += 1;
+    st->qAq = tot;
+    if (!(tot > 0.0)) {
+      st->done = 1;
+      st->status = (tot <= 0.0) ? ST_BREAKDOWN : ST_NONFINITE;
+    } else {
+      st->alpha = st->rz / tot;
+      st->alpha_f = (float)st->alpha;
+      st->neg_alpha_f = (float)(-st->alpha);
+    }
+  }
+}
+
+// x += alpha q; r_new = r - alpha Ap (r kept as r_prev); rel = max|r_new|/bnorm
+// (pfflip/poisson.py:390-398)
+__global__ void __launch_bounds__(RED_NT) k_update_xr(long long n, const float* __restrict__ q,
+                                                      const float* __restrict__ Ap, const float* __restrict__ r,
+                                                      float* __restrict__ r_new, float* __restrict__ x,
+                                                      double* partials, unsigned* counter, MGState* st) {
+  if (is_done(st)) return;
+  __shared__ float shf[40];
+  const float af = st->alpha_f, naf = st->neg_alpha_f;
+  float m = 0.f;
+  for (long long e = blockIdx.x * (long long)RED_NT + threadIdx.x; e < n; e += (long long)gridDim.x * RED_NT) {
+    x[e] += af * q[e];
+    const float v = r[e] + naf * Ap[e];
+    r_new[e] = v;
+    m = fmaxf(m, isfinite(v) ? fabsf(v) : INFINITY);
+  }
+  m = block_max<RED_NT>(m, shf);
+  float tot;
+  if (grid_max_last<RED_NT>(m, partials, counter, &tot, shf) && threadIdx.x == 0) {
+    const double rel = (double)tot / st->bnorm;
+    st->rel = rel;
+    st->maxabs_last = tot;
+    if (!(rel == rel) || isinf(rel)) {
+      st->done = 1;
+      st->status = ST_NONFINITE;
+    } else if (rel < (double)st->tol) {
+      st->done = 1;
+      st->status = ST_CONVERGED;
+    }
+    int ex = 0;
+    frexpf(tot > 0.f ? tot : 1.f, &ex);
+    st->scale_r = ldexpf(1.f, -ex);
+  }
+}
+
+// rz_new = <r, z>, rpz = <r_prev, z>, beta = max((rz_new - rpz)/rz, 0), rz = rz_new
+// (pfflip/poisson.py:402-406)
+template <class T>
+__global__ void __launch_bounds__(RED_NT) k_dots(long long n, const T* __restrict__ p, const float* __restrict__ r,
+                                                 const float* __restrict__ r_prev, double* partials,
+                                                 unsigned* counter, MGState* st, int mixed) {
+  if (is_done(st)) return;
+  __shared__ double sh[40];
+  const float c = st->c_shift, zs = mixed ? st->zscale : 1.f;
+  double s1 = 0.0, s2 = 0.0;
+  for (long long e = blockIdx.x * (long long)RED_NT + threadIdx.x; e < n; e += (long long)gridDim.x * RED_NT) {
+    const double z = (double)zval(p, e, zs, c);
+    s1 += (double)r[e] * z;
+    s2 += (double)r_prev[e] * z;
+  }
+  s1 = block_sum<RED_NT>(s1, sh);
+  s2 = block_sum<RED_NT>(s2, sh);
+  double t1, t2;
+  if (grid_sum2_last<RED_NT>(s1, s2, partials, counter, &t1, &t2, sh) && threadIdx.x == 0) {
+    const double num = t1 - t2;
+    const double beta = (st->rz != 0.0) ? fmax(num / st->rz, 0.0) : 0.0;
+    st->rz_new = t1;
+    st->rpz = t2;
+    st->beta = beta;
+    st->beta_f = (float)beta;
+    st->rz = t1;
+  }
+}
+
+// q = z + beta q   (pfflip/poisson.py:405, scale_add)
+template <class T>
+__global__ void __launch_bounds__(RED_NT) k_update_q(long long n, const T* __restrict__ p, float* __restrict__ q,
+                                                     MGState* st, int mixed) {
+  if (is_done(st)) return;
+  const float c = st->c_shift, zs = mixed ? st->zscale : 1.f, bf = st->beta_f;
+  for (long long e = blockIdx.x * (long long)RED_NT + threadIdx.x; e < n; e += (long long)gridDim.x * RED_NT)
+    q[e] = zval(p, e, zs, c) + bf * q[e];
+}
+
+// z = p*zscale + c_shift written out (precondition entry point)
+template <class T>
+__global__ void k_write_z(long long n, const T* __restrict__ p, float* __restrict__ z, const MGState* st, int mixed) {
+  const float c = st->c_shift, zs = mixed ? st->zscale : 1.f;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    z[e] = zval(p, e, zs, c);
+}
+
+// final mean removal of x written into the caller's output (pfflip/poisson.py:408)
+__global__ void k_shift_out(long long n, const float* __restrict__ x, float* __restrict__ out, const MGState* st) {
+  const float c = st->c_shift;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    out[e] = x[e] + c;
+}
+
+__global__ void k_set_state(MGState* st, float tol, int max_iter, float zscale_base) {
+  st->tol = tol;
+  st->max_iter = max_iter;
+  st->done = 0;
+  st->status = ST_RUNNING;
+  st->it = 0;
+  st->rel = 1.0;
+  st->zscale = zscale_base;  // multiplied by 1/scale_r where used
+}
+
+// zscale = zscale_base / scale_r (16-bit hierarchy)
+__global__ void k_update_zscale(MGState* st, float coef_scale) {
+  st->zscale = coef_scale / st->scale_r;
+}
+
+__global__ void k_copy_f(long long n, const float* __restrict__ a, float* __restrict__ b) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    b[e] = a[e];
+}
+
+
+// generic mean of a level-0 vector stored as T: c_shift = float(-mean * zscale)
+template <class T>
+__global__ void __launch_bounds__(RED_NT) k_mean_of(long long n, const T* __restrict__ p, double* partials,
+                                                    unsigned* counter, MGState* st, int mixed) {
+  __shared__ double sh[40];
+  double s = 0.0;
+  for (long long e = blockIdx.x * (long long)RED_NT + threadIdx.x; e < n; e += (long long)gridDim.x * RED_NT)
+    s += (double)ldT(p + e);
+  s = block_sum<RED_NT>(s, sh);
+  double tot;
+  if (grid_sum_last<RED_NT>(s, partials, counter, &tot, sh) && threadIdx.x == 0) {
+    st->sum_last = tot;
+    st->c_shift = (float)(-(tot / (double)n) * (mixed ? (double)st->zscale : 1.0));
+  }
+}
+
+// p += float(-mean(p)) in place (mean from st->sum_last; coarsest-level fallback)
+template <class T>
+__global__ void k_shift_mean_inplace(long long n, T* __restrict__ p, const MGState* st) {
+  const float c = (float)(-(st->sum_last / (double)n));
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    stT(p + e, ldT(p + e) + c);
+}
+
+// fine p += pscale * coarse p[i/2, j/2, k/2]   (pfflip/poisson.py:178-182)
+template <class T>
+__global__ void k_prolong_add(int n0, int n1, int n2, const T* __restrict__ pc, T* __restrict__ p, float pscale,
+                              const MGState* st) {
+  if (is_done(st)) return;
+  const long long n = (long long)n0 * n1 * n2;
+  const int h1 = n1 >> 1, h2 = n2 >> 1;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(e % n2);
+    const long long t = e / n2;
+    const int j = (int)(t % n1), i = (int)(t / n1);
+    stT(p + e, ldT(p + e) + ldT(pc + ((long long)(i >> 1) * h1 + (j >> 1)) * h2 + (k >> 1)) * pscale);
+  }
+}
+
+// max|r| -> scale_r and zscale (precondition entry point, 16-bit hierarchy)
+__global__ void __launch_bounds__(RED_NT) k_scale_of(long long n, const float* __restrict__ r, double* partials,
+                                                     unsigned* counter, MGState* st, float coef_scale) {
+  __shared__ float shf[40];
+  float m = 0.f;
+  for (long long e = blockIdx.x * (long long)RED_NT + threadIdx.x; e < n; e += (long long)gridDim.x * RED_NT)
+    m = fmaxf(m, fabsf(r[e]));
+  m = block_max<RED_NT>(m, shf);
+  float tot;
+  if (grid_max_last<RED_NT>(m, partials, counter, &tot, shf) && threadIdx.x == 0) {
+    int ex = 0;
+    frexpf(tot > 0.f && isfinite(tot) ? tot : 1.f, &ex);
+    st->scale_r = ldexpf(1.f, -ex);
+    st->zscale = coef_scale / st->scale_r;
+  }
+}
+
+__global__ void k_clear_done(MGState* st) {
+  st->done = 0;
+  st->status = ST_RUNNING;
+}
+
+// coarsest level in one CTA, b possibly of another storage type (level 0)
+template <class T, class TB, class AccT>
+__global__ void __launch_bounds__(CO_NT) k_coarsest_b(int n0, int n1, int n2, const TB* __restrict__ b,
+                                                      const float* b_scale, const T* __restrict__ bx,
+                                                      const T* __restrict__ by, const T* __restrict__ bz,
+                                                      T* __restrict__ p_out, int sweeps, float omega, MGState* st,
+                                                      int flux) {
+  if (is_done(st)) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int n = n0 * n1 * n2;
+  const int nfx = (n0 + 1) * n1 * n2, nfy = n0 * (n1 + 1) * n2, nfz = n0 * n1 * (n2 + 1);
+  AccT* P = reinterpret_cast<AccT*>(smraw);
+  AccT* B = P + n;
+  AccT* D = B + n;
+  float* X = reinterpret_cast<float*>(D + n);
+  float* Y = X + nfx;
+  float* Z = Y + nfy;
+  __shared__ double sred[40];
+  const int tid = threadIdx.x;
+  const float bsc = b_scale ? *b_scale : 1.f;
+  for (int e = tid; e < n; e += CO_NT) { P[e] = AccT(0); B[e] = (AccT)(ldT(b + e) * bsc); }
+  for (int e = tid; e < nfx; e += CO_NT) X[e] = ldT(bx + e);
+  for (int e = tid; e < nfy; e += CO_NT) Y[e] = ldT(by + e);
+  for (int e = tid; e < nfz; e += CO_NT) Z[e] = ldT(bz + e);
+  __syncthreads();
+  const int sI = n1 * n2;
+  for (int e = tid; e < n; e += CO_NT) {
+    const int k = e % n2, t = e / n2, j = t % n1, i = t / n1;
+    const int fyi = (i * (n1 + 1) + j) * n2 + k, fzi = (i * n1 + j) * (n2 + 1) + k;
+    D[e] = (AccT)(X[e] + X[e + sI] + Y[fyi] + Y[fyi + n2] + Z[fzi] + Z[fzi + 1]);
+  }
+  __syncthreads();
+  const AccT om = (AccT)omega;
+  for (int s = 0; s < sweeps; ++s) {
+    for (int color = 0; color < 2; ++color) {
+      for (int e = tid; e < n; e += CO_NT) {
+        const int k = e % n2, t = e / n2, j = t % n1, i = t / n1;
+        if (((i + j + k) & 1) != color) continue;
+        const AccT d = D[e];
+        if (!(d > AccT(0))) continue;
+        const int fyi = (i * (n1 + 1) + j) * n2 + k, fzi = (i * n1 + j) * (n2 + 1) + k;
+        const AccT pv = P[e];
+        const AccT q0 = P[i > 0 ? e - sI : e], q1 = P[i < n0 - 1 ? e + sI : e];
+        const AccT q2 = P[j > 0 ? e - n2 : e], q3 = P[j < n1 - 1 ? e + n2 : e];
+        const AccT q4 = P[k > 0 ? e - 1 : e], q5 = P[k < n2 - 1 ? e + 1 : e];
+        AccT res;
+        if (flux) {
+          AccT sum = (AccT)X[e] * (pv - q0);
+          sum += (AccT)X[e + sI] * (pv - q1);
+          sum += (AccT)Y[fyi] * (pv - q2);
+          sum += (AccT)Y[fyi + n2] * (pv - q3);
+          sum += (AccT)Z[fzi] * (pv - q4);
+          sum += (AccT)Z[fzi + 1] * (pv - q5);
+          res = B[e] - sum;
+        } else {
+          AccT sum = (AccT)X[e] * q0;
+          sum += (AccT)X[e + sI] * q1;
+          sum += (AccT)Y[fyi] * q2;
+          sum += (AccT)Y[fyi + n2] * q3;
+          sum += (AccT)Z[fzi] * q4;
+          sum += (AccT)Z[fzi + 1] * q5;
+          res = B[e] - (d * pv - sum);
+        }
+        P[e] += om * res / d;
+      }
+      __syncthreads();
+    }
+  }
+  double ls = 0.0;
+  for (int e = tid; e < n; e += CO_NT) ls += (double)P[e];
+  const double tot = block_sum<CO_NT>(ls, sred);
+  __shared__ double s_mean;
+  if (tid == 0) s_mean = tot / (double)n;
+  __syncthreads();
+  const AccT shift = (AccT)(-s_mean);
+  for (int e = tid; e < n; e += CO_NT) stT(p_out + e, (float)(P[e] + shift));
+}
+
+// =============================================================== host side
+void count_suppress(bool on);
+
+}  // namespace pf
+
+struct pf_mg_plan {
+  pf_mg_desc d;
+  int prec;
+  float lp_scale[PF_MG_MAX_LEVELS];
+  int ci[PF_MG_MAX_LEVELS];
+  cudaStream_t cap_stream;
+  cudaGraphExec_t exec[2];
+  size_t exec_nodes[2];
+  bool graphs_ready;
+  pf::MGState* h_state[2];
+  cudaEvent_t ev[2];
+};
+
+namespace {
+using namespace pf;
+
+inline MGState* ST(pf_mg_plan* P) { return reinterpret_cast<MGState*>(P->d.state); }
+inline unsigned* CNT(pf_mg_plan* P, int k) { return P->d.counters + k; }
+inline float* scale_r_ptr(pf_mg_plan* P) { return &ST(P)->scale_r; }
+inline long long ncells(const pf_mg_level& L) { return (long long)L.nx * L.ny * L.nz; }
+inline bool mixed(const pf_mg_plan* P) { return P->prec != PF_PREC_FP32; }
+inline int FLUX(const pf_mg_plan* P) { return P->d.stencil == PF_STENCIL_FLUX ? 1 : 0; }
+
+template <class T> struct LV { T *bx, *by, *bz, *p0, *p1, *b; };
+
+template <class T> LV<T> view(pf_mg_plan* P, int lv) {
+  const pf_mg_level& L = P->d.lev[lv];
+  if (P->prec == PF_PREC_FP32)
+    return LV<T>{(T*)L.bx, (T*)L.by, (T*)L.bz, (T*)L.p, (T*)L.p_alt, (T*)L.b};
+  return LV<T>{(T*)L.bx_lp, (T*)L.by_lp, (T*)L.bz_lp, (T*)L.p_lp, (T*)L.p_lp_alt, (T*)L.b_lp};
+}
+
+int red_grid(long long n) { return grid_for(n, RED_NT, RED_MAX_BLOCKS); }
+int ew_grid(long long n) { return grid_for(n, 256, kNumSMs * 16); }
+
+template <class T, class TB>
+int launch_sweep(pf_mg_plan* P, int lv, const T* p_in, bool zero_in, T* p_out, const TB* b, const float* b_scale,
+                 const LV<T>& V, const T* pc, float pc_scale, int first_color, bool mean, bool use_state,
+                 cudaStream_t s) {
+  const pf_mg_level& L = P->d.lev[lv];
+  SweepArgs<T, TB> a;
+  a.n0 = L.nx; a.n1 = L.ny; a.n2 = L.nz;
+  a.ci = P->ci[lv];
+  a.p_in = p_in; a.zero_in = zero_in ? 1 : 0; a.p_out = p_out;
+  a.b = b; a.b_scale = b_scale;
+  a.bx = V.bx; a.by = V.by; a.bz = V.bz;
+  a.pc = pc; a.pc_scale = pc_scale;
+  a.omega = P->d.omega;
+  a.first_color = first_color;
+  a.partials = mean ? P->d.partials : nullptr;
+  a.counter = CNT(P, CNT_SWEEP_MEAN);
+  a.st = use_state ? ST(P) : nullptr;
+  a.n_total = (int)ncells(L);
+  a.mixed = mixed(P) ? 1 : 0;
+  a.flux = P->d.stencil == PF_STENCIL_FLUX ? 1 : 0;
+  dim3 grid((L.nz + SW_TK - 1) / SW_TK, (L.ny + SW_TJ - 1) / SW_TJ, (L.nx + a.ci - 1) / a.ci);
+  k_rb_sweep<T, TB><<<grid, SW_NT, 0, s>>>(a);
+  PF_LAUNCHED();
+  return PF_OK;
+}
+
+size_t coarsest_smem(const pf_mg_level& L, size_t acc) {
+  const size_t n = (size_t)L.nx * L.ny * L.nz;
+  const size_t nf = (size_t)(L.nx + 1) * L.ny * L.nz + (size_t)L.nx * (L.ny + 1) * L.nz + (size_t)L.nx * L.ny * (L.nz + 1);
+  return n * 3 * acc + nf * sizeof(float);
+}
+
+#define PF_TRY(x)              \
+  do {                         \
+    int rc_ = (x);             \
+    if (rc_ != PF_OK) return rc_; \
+  } while (0)
+
+// One V-cycle on level lv with right-hand side b (storage TB, times *b_scale);
+// the level's final p is returned in *out.  want_mean: the mean of the final p
+// goes to st->c_shift (level 0 only).
+template <class T, class TB>
+int vcycle(pf_mg_plan* P, int lv, const TB* b, const float* b_scale, bool want_mean, cudaStream_t s, T** out) {
+  const pf_mg_level& L = P->d.lev[lv];
+  LV<T> V = view<T>(P, lv);
+  const int nlev = P->d.nlev;
+  const long long n = ncells(L);
+  if (lv == nlev - 1) {
+    T* res = V.p0;
+    if (n <= kCoarseMaxCells) {
+      if (mixed(P)) {
+        k_coarsest_b<T, TB, double><<<1, CO_NT, coarsest_smem(L, sizeof(double)), s>>>(
+            L.nx, L.ny, L.nz, b, b_scale, V.bx, V.by, V.bz, res, P->d.coarsest, P->d.omega, ST(P), FLUX(P));
+      } else {
+        k_coarsest_b<T, TB, float><<<1, CO_NT, coarsest_smem(L, sizeof(float)), s>>>(
+            L.nx, L.ny, L.nz, b, b_scale, V.bx, V.by, V.bz, res, P->d.coarsest, P->d.omega, ST(P), FLUX(P));
+      }
+      PF_LAUNCHED();
+    } else {
+      T* cur = nullptr;
+      for (int it = 0; it < P->d.coarsest; ++it) {
+        T* o = (it & 1) ? V.p1 : V.p0;
+        PF_TRY((launch_sweep<T, TB>(P, lv, cur, it == 0, o, b, b_scale, V, nullptr, 1.f, 0, false, true, s)));
+        cur = o;
+      }
+      if (!cur) {
+        PF_CUDA_TRY(cudaMemsetAsync(V.p0, 0, sizeof(T) * n, s));
+        cur = V.p0;
+      }
+      k_mean_of<T><<<red_grid(n), RED_NT, 0, s>>>(n, cur, P->d.partials, CNT(P, CNT_COARSE), ST(P), 0);
+      PF_LAUNCHED();
+      k_shift_mean_inplace<T><<<ew_grid(n), 256, 0, s>>>(n, cur, ST(P));
+      PF_LAUNCHED();
+      res = cur;
+    }
+    if (want_mean) {
+      k_mean_of<T><<<red_grid(n), RED_NT, 0, s>>>(n, res, P->d.partials, CNT(P, CNT_SWEEP_MEAN), ST(P),
+                                                  mixed(P) ? 1 : 0);
+      PF_LAUNCHED();
+    }
+    *out = res;
+    return PF_OK;
+  }
+  const float rscale = mixed(P) ? 0.125f : 1.f;
+  const float pscale = mixed(P) ? 2.f : 1.f;
+  T* cur = nullptr;
+  for (int it = 0; it < P->d.pre; ++it) {
+    T* o = (it & 1) ? V.p1 : V.p0;
+    PF_TRY((launch_sweep<T, TB>(P, lv, cur, it == 0, o, b, b_scale, V, nullptr, 1.f, 0, false, true, s)));
+    cur = o;
+  }
+  if (!cur) {
+    PF_CUDA_TRY(cudaMemsetAsync(V.p0, 0, sizeof(T) * n, s));
+    cur = V.p0;
+  }
+  LV<T> C = view<T>(P, lv + 1);
+  const pf_mg_level& CL = P->d.lev[lv + 1];
+  k_residual_restrict<T, TB><<<ew_grid(ncells(CL)), 256, 0, s>>>(L.nx, L.ny, L.nz, cur, b, b_scale, V.bx, V.by,
+                                                                V.bz, C.b, rscale, nullptr, ST(P), FLUX(P));
+  PF_LAUNCHED();
+  T* pc = nullptr;
+  PF_TRY((vcycle<T, T>(P, lv + 1, C.b, nullptr, false, s, &pc)));
+  if (P->d.post == 0) {
+    k_prolong_add<T><<<ew_grid(n), 256, 0, s>>>(L.nx, L.ny, L.nz, pc, cur, pscale, ST(P));
+    PF_LAUNCHED();
+    if (want_mean) {
+      k_mean_of<T><<<red_grid(n), RED_NT, 0, s>>>(n, cur, P->d.partials, CNT(P, CNT_SWEEP_MEAN), ST(P),
+                                                  mixed(P) ? 1 : 0);
+      PF_LAUNCHED();
+    }
+  } else {
+    for (int it = 0; it < P->d.post; ++it) {
+      T* o = (cur == V.p0) ? V.p1 : V.p0;
+      PF_TRY((launch_sweep<T, TB>(P, lv, cur, false, o, b, b_scale, V, it == 0 ? pc : nullptr, pscale, 1,
+                                  want_mean && it == P->d.post - 1, true, s)));
+      cur = o;
+    }
+  }
+  *out = cur;
+  return PF_OK;
+}
+
+template <class T> int vcycle0(pf_mg_plan* P, const float* r, cudaStream_t s, T** out) {
+  return vcycle<T, float>(P, 0, r, mixed(P) ? scale_r_ptr(P) : nullptr, true, s, out);
+}
+
+template <class T> int enqueue_setup(pf_mg_plan* P, const float* b, float tol, int max_iter, cudaStream_t s) {
+  const pf_mg_level& L0 = P->d.lev[0];
+  const long long n = ncells(L0);
+  k_set_state<<<1, 1, 0, s>>>(ST(P), tol, max_iter, P->d.coef_scale);
+  PF_LAUNCHED();
+  k_sum_mean<<<red_grid(n), RED_NT, 0, s>>>(n, b, P->d.partials, CNT(P, CNT_SUM_B), ST(P));
+  PF_LAUNCHED();
+  k_init_r<<<red_grid(n), RED_NT, 0, s>>>(n, b, P->d.rhs, P->d.res_v, P->d.x, P->d.partials, CNT(P, CNT_INIT_R),
+                                          ST(P));
+  PF_LAUNCHED();
+  if (mixed(P)) {
+    k_update_zscale<<<1, 1, 0, s>>>(ST(P), P->d.coef_scale);
+    PF_LAUNCHED();
+  }
+  T* p0 = nullptr;
+  PF_TRY(vcycle0<T>(P, P->d.res_v, s, &p0));
+  k_init_q<T><<<red_grid(n), RED_NT, 0, s>>>(n, p0, P->d.res_v, P->d.q, P->d.z, P->d.partials, CNT(P, CNT_INIT_Q),
+                                             ST(P), mixed(P) ? 1 : 0);
+  PF_LAUNCHED();
+  return PF_OK;
+}
+
+template <class T> int enqueue_iteration(pf_mg_plan* P, int par, cudaStream_t s) {
+  const pf_mg_level& L0 = P->d.lev[0];
+  const long long n = ncells(L0);
+  float* r_cur = par ? P->d.res_alt : P->d.res_v;
+  float* r_new = par ? P->d.res_v : P->d.res_alt;
+  k_apply_dot<<<red_grid(n), RED_NT, 0, s>>>(L0.nx, L0.ny, L0.nz, P->d.q, L0.bx, L0.by, L0.bz, nullptr, P->d.Ap,
+                                             P->d.partials, CNT(P, CNT_APPLY_DOT), ST(P), FLUX(P));
+  PF_LAUNCHED();
+  k_update_xr<<<red_grid(n), RED_NT, 0, s>>>(n, P->d.q, P->d.Ap, r_cur, r_new, P->d.x, P->d.partials,
+                                             CNT(P, CNT_UPDATE_XR), ST(P));
+  PF_LAUNCHED();
+  if (mixed(P)) {
+    k_update_zscale<<<1, 1, 0, s>>>(ST(P), P->d.coef_scale);
+    PF_LAUNCHED();
+  }
+  T* p0 = nullptr;
+  PF_TRY(vcycle0<T>(P, r_new, s, &p0));
+  k_dots<T><<<red_grid(n), RED_NT, 0, s>>>(n, p0, r_new, r_cur, P->d.partials, CNT(P, CNT_DOTS), ST(P),
+                                           mixed(P) ? 1 : 0);
+  PF_LAUNCHED();
+  k_update_q<T><<<ew_grid(n), RED_NT, 0, s>>>(n, p0, P->d.q, ST(P), mixed(P) ? 1 : 0);
+  PF_LAUNCHED();
+  return PF_OK;
+}
+
+int enqueue_final(pf_mg_plan* P, float* x_out, cudaStream_t s) {
+  const long long n = ncells(P->d.lev[0]);
+  k_sum_mean<<<red_grid(n), RED_NT, 0, s>>>(n, P->d.x, P->d.partials, CNT(P, CNT_FINAL_SUM), ST(P));
+  PF_LAUNCHED();
+  k_shift_out<<<ew_grid(n), 256, 0, s>>>(n, P->d.x, x_out, ST(P));
+  PF_LAUNCHED();
+  return PF_OK;
+}
+
+template <class T> int capture_graphs(pf_mg_plan* P) {
+  for (int par = 0; par < 2; ++par) {
+    cudaGraph_t g = nullptr;
+    PF_CUDA_TRY(cudaStreamBeginCapture(P->cap_stream, cudaStreamCaptureModeThreadLocal));
+    count_suppress(true);
+    int rc = enqueue_iteration<T>(P, par, P->cap_stream);
+    count_suppress(false);
+    cudaError_t e = cudaStreamEndCapture(P->cap_stream, &g);
+    if (rc != PF_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) {
+      set_cuda_error(e, "cudaStreamEndCapture");
+      return PF_ERR_CUDA;
+    }
+    size_t nn = 0;
+    cudaGraphGetNodes(g, nullptr, &nn);
+    P->exec_nodes[par] = nn;
+    e = cudaGraphInstantiate(&P->exec[par], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      set_cuda_error(e, "cudaGraphInstantiate");
+      return PF_ERR_CUDA;
+    }
+  }
+  P->graphs_ready = true;
+  return PF_OK;
+}
+
+template <class T>
+int solve_impl(pf_mg_plan* P, const float* b, float* x, float tol, int max_iter, int use_graphs, int verbose,
+               int* iters_out, double* rel_out, cudaStream_t s) {
+  PF_TRY(enqueue_setup<T>(P, b, tol, max_iter, s));
+  if (use_graphs && !P->graphs_ready) PF_TRY(capture_graphs<T>(P));
+  for (int k = 1; k <= max_iter; ++k) {
+    const int par = (k - 1) & 1;
+    if (use_graphs) {
+      PF_CUDA_TRY(cudaGraphLaunch(P->exec[par], s));
+      count_launch(P->exec_nodes[par]);
+    } else {
+      PF_TRY(enqueue_iteration<T>(P, par, s));
+    }
+    PF_CUDA_TRY(cudaMemcpyAsync(P->h_state[k & 1], P->d.state, sizeof(MGState), cudaMemcpyDeviceToHost, s));
+    PF_CUDA_TRY(cudaEventRecord(P->ev[k & 1], s));
+    if (verbose) {
+      PF_CUDA_TRY(cudaEventSynchronize(P->ev[k & 1]));
+      const MGState* h = P->h_state[k & 1];
+      if (h->it == k) std::printf("    pcg it=%3d  |r|inf/|b|inf = %.3e\n", h->it, h->rel);
+      if (h->done) break;
+      continue;
+    }
+    if (k >= 2) {
+      PF_CUDA_TRY(cudaEventSynchronize(P->ev[(k - 1) & 1]));
+      if (P->h_state[(k - 1) & 1]->done) break;
+    }
+  }
+  PF_TRY(enqueue_final(P, x, s));
+  PF_CUDA_TRY(cudaMemcpyAsync(P->h_state[0], P->d.state, sizeof(MGState), cudaMemcpyDeviceToHost, s));
+  PF_CUDA_TRY(cudaStreamSynchronize(s));
+  const MGState* h = P->h_state[0];
+  *iters_out = h->it;
+  *rel_out = h->rel;
+  if (h->status == ST_NONFINITE) {
+    set_error(PF_ERR_NONFINITE, "non-finite residual in the CG iteration %d", h->it);
+    return PF_ERR_NONFINITE;
+  }
+  if (h->status == ST_RUNNING) {
+    set_error(PF_ERR_NOT_CONVERGED, "tolerance %g not reached in %d iterations (rel %g)", (double)tol, h->it, h->rel);
+    return PF_ERR_NOT_CONVERGED;
+  }
+  return PF_OK;
+}
+
+template <class T> int build_impl(pf_mg_plan* P, cudaStream_t s) {
+  for (int lv = 0; lv < P->d.nlev; ++lv) {
+    const pf_mg_level& L = P->d.lev[lv];
+    const long long n = ncells(L);
+    const long long nf = (long long)(L.nx + 1) * L.ny * L.nz + (long long)L.nx * (L.ny + 1) * L.nz +
+                         (long long)L.nx * L.ny * (L.nz + 1);
+    T* lpx = mixed(P) ? (T*)L.bx_lp : nullptr;
+    k_level_coefs<T><<<ew_grid(n + (lpx ? nf : 0)), 256, 0, s>>>(L.nx, L.ny, L.nz, L.bx, L.by, L.bz, L.diag, lpx,
+                                                                 (T*)L.by_lp, (T*)L.bz_lp, P->lp_scale[lv]);
+    PF_LAUNCHED();
+    if (lv + 1 < P->d.nlev) {
+      const pf_mg_level& C = P->d.lev[lv + 1];
+      const long long ncf = (long long)(C.nx + 1) * C.ny * C.nz + (long long)C.nx * (C.ny + 1) * C.nz +
+                            (long long)C.nx * C.ny * (C.nz + 1);
+      k_coarsen_faces<<<ew_grid(ncf), 256, 0, s>>>(L.nx, L.ny, L.nz, C.nx, C.ny, C.nz, L.bx, L.by, L.bz, C.bx, C.by,
+                                                    C.bz);
+      PF_LAUNCHED();
+    }
+  }
+  return PF_OK;
+}
+
+template <class T> int precondition_impl(pf_mg_plan* P, const float* r, float* z, cudaStream_t s) {
+  const long long n = ncells(P->d.lev[0]);
+  k_clear_done<<<1, 1, 0, s>>>(ST(P));
+  PF_LAUNCHED();
+  if (mixed(P)) {
+    k_scale_of<<<red_grid(n), RED_NT, 0, s>>>(n, r, P->d.partials, CNT(P, CNT_SCALE), ST(P), P->d.coef_scale);
+    PF_LAUNCHED();
+  }
+  T* p0 = nullptr;
+  PF_TRY(vcycle0<T>(P, r, s, &p0));
+  k_write_z<T><<<ew_grid(n), 256, 0, s>>>(n, p0, z, ST(P), mixed(P) ? 1 : 0);
+  PF_LAUNCHED();
+  return PF_OK;
+}
+
+template <class T> void set_smem_attrs() {
+  const int mx = 200 * 1024;
+  cudaFuncSetAttribute(k_coarsest_b<T, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_coarsest_b<T, T, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_coarsest_b<T, float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_coarsest_b<T, T, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+}
+
+}  // namespace
+
+extern "C" {
+
+int64_t pf_mg_partials_count(void) { return pf::kPartials; }
+
+int32_t pf_mg_level_count(int32_t nx, int32_t ny, int32_t nz, int32_t min_dim, int32_t* dims_out) {
+  int r[3] = {nx, ny, nz};
+  int n = 0;
+  while (n < PF_MG_MAX_LEVELS) {
+    if (dims_out) { dims_out[3 * n] = r[0]; dims_out[3 * n + 1] = r[1]; dims_out[3 * n + 2] = r[2]; }
+    ++n;
+    const int mn = r[0] < r[1] ? (r[0] < r[2] ? r[0] : r[2]) : (r[1] < r[2] ? r[1] : r[2]);
+    if (mn / 2 < min_dim || (r[0] % 2) || (r[1] % 2) || (r[2] % 2)) break;
+    r[0] /= 2; r[1] /= 2; r[2] /= 2;
+  }
+  return n;
+}
+
+int pf_mg_plan_create(const pf_mg_desc* desc, pf_mg_plan** out) {
+  PF_REQUIRE(desc && out, "null argument");
+  PF_REQUIRE(desc->nlev >= 1 && desc->nlev <= PF_MG_MAX_LEVELS, "nlev %d out of range", desc->nlev);
+  PF_REQUIRE(desc->precision >= PF_PREC_FP32 && desc->precision <= PF_PREC_BF16, "bad precision");
+  PF_REQUIRE(desc->stencil == PF_STENCIL_REFERENCE || desc->stencil == PF_STENCIL_FLUX, "bad stencil");
+  PF_REQUIRE(desc->state && desc->partials && desc->counters, "state/partials/counters required");
+  PF_REQUIRE(desc->res_v && desc->res_alt && desc->q && desc->Ap && desc->x, "CG vectors required");
+  for (int lv = 0; lv < desc->nlev; ++lv) {
+    const pf_mg_level& L = desc->lev[lv];
+    PF_REQUIRE(L.nx > 0 && L.ny > 0 && L.nz > 0, "level %d dims", lv);
+    PF_REQUIRE(L.bx && L.by && L.bz && L.diag && L.p && L.p_alt && L.b, "level %d fp32 arrays", lv);
+    if (desc->precision != PF_PREC_FP32)
+      PF_REQUIRE(L.bx_lp && L.by_lp && L.bz_lp && L.p_lp && L.p_lp_alt && L.b_lp, "level %d 16-bit arrays", lv);
+    if (lv > 0) {
+      const pf_mg_level& F = desc->lev[lv - 1];
+      PF_REQUIRE(F.nx == 2 * L.nx && F.ny == 2 * L.ny && F.nz == 2 * L.nz, "level %d is not half of level %d", lv,
+                 lv - 1);
+    }
+    const long long tiles = (long long)((L.nz + SW_TK - 1) / SW_TK) * ((L.ny + SW_TJ - 1) / SW_TJ);
+    PF_REQUIRE(tiles <= pf::kPartials, "level %d too large for the sweep reduction", lv);
+  }
+  pf_mg_plan* P = new pf_mg_plan();
+  std::memset(P, 0, sizeof(*P));
+  P->d = *desc;
+  P->prec = desc->precision;
+  for (int lv = 0; lv < desc->nlev; ++lv) {
+    const pf_mg_level& L = desc->lev[lv];
+    P->lp_scale[lv] = std::ldexp(desc->coef_scale > 0.f ? desc->coef_scale : 1.f, -2 * lv);
+    const long long tiles = (long long)((L.nz + SW_TK - 1) / SW_TK) * ((L.ny + SW_TJ - 1) / SW_TJ);
+    long long ci = (L.nx * tiles + 443) / 444;
+    if (ci < 4) ci = 4;
+    long long chunks = (L.nx + ci - 1) / ci;
+    while (tiles * chunks > pf::kPartials) { ci *= 2; chunks = (L.nx + ci - 1) / ci; }
+    P->ci[lv] = (int)ci;
+  }
+  cudaError_t e = cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaHostAlloc((void**)&P->h_state[0], sizeof(pf::MGState) * 2, cudaHostAllocDefault);
+  if (e == cudaSuccess) {
+    P->h_state[1] = P->h_state[0] + 1;
+    e = cudaEventCreateWithFlags(&P->ev[0], cudaEventDisableTiming);
+  }
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev[1], cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    pf::set_cuda_error(e, "pf_mg_plan_create");
+    pf_mg_plan_destroy(P);
+    return PF_ERR_CUDA;
+  }
+  set_smem_attrs<float>();
+  set_smem_attrs<__half>();
+  set_smem_attrs<__nv_bfloat16>();
+  *out = P;
+  return PF_OK;
+}
+
+int pf_mg_plan_destroy(pf_mg_plan* P) {
+  if (!P) return PF_OK;
+  for (int i = 0; i < 2; ++i) {
+    if (P->exec[i]) cudaGraphExecDestroy(P->exec[i]);
+    if (P->ev[i]) cudaEventDestroy(P->ev[i]);
+  }
+  if (P->h_state[0]) cudaFreeHost(P->h_state[0]);
+  if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
+  delete P;
+  return PF_OK;
+}
+
+int pf_mg_build_hierarchy(pf_mg_plan* P, const float* bx, const float* by, const float* bz, void* stream) {
+  PF_REQUIRE(P && bx && by && bz, "null argument");
+  cudaStream_t s = S(stream);
+  const pf_mg_level& L0 = P->d.lev[0];
+  const size_t nfx = (size_t)(L0.nx + 1) * L0.ny * L0.nz, nfy = (size_t)L0.nx * (L0.ny + 1) * L0.nz,
+               nfz = (size_t)L0.nx * L0.ny * (L0.nz + 1);
+  if (bx != L0.bx) PF_CUDA_TRY(cudaMemcpyAsync(L0.bx, bx, nfx * 4, cudaMemcpyDeviceToDevice, s));
+  if (by != L0.by) PF_CUDA_TRY(cudaMemcpyAsync(L0.by, by, nfy * 4, cudaMemcpyDeviceToDevice, s));
+  if (bz != L0.bz) PF_CUDA_TRY(cudaMemcpyAsync(L0.bz, bz, nfz * 4, cudaMemcpyDeviceToDevice, s));
+  switch (P->prec) {
+    case PF_PREC_FP16: return build_impl<__half>(P, s);
+    case PF_PREC_BF16: return build_impl<__nv_bfloat16>(P, s);
+    default: return build_impl<float>(P, s);
+  }
+}
+
+int pf_mg_precondition(pf_mg_plan* P, const float* r, float* z, void* stream) {
+  PF_REQUIRE(P && r && z, "null argument");
+  switch (P->prec) {
+    case PF_PREC_FP16: return precondition_impl<__half>(P, r, z, S(stream));
+    case PF_PREC_BF16: return precondition_impl<__nv_bfloat16>(P, r, z, S(stream));
+    default: return precondition_impl<float>(P, r, z, S(stream));
+  }
+}
+
+int pf_mg_smooth(pf_mg_plan* P, int32_t lv, int32_t nsweeps, int32_t reverse, void* stream) {
+  PF_REQUIRE(P && lv >= 0 && lv < P->d.nlev && nsweeps >= 0, "bad argument");
+  cudaStream_t s = S(stream);
+  const pf_mg_level& L = P->d.lev[lv];
+  LV<float> V{L.bx, L.by, L.bz, L.p, L.p_alt, L.b};
+  const int saved = P->prec;
+  P->prec = PF_PREC_FP32;  // this entry point runs on the fp32 level arrays
+  float* cur = L.p;
+  int rc = PF_OK;
+  for (int it = 0; it < nsweeps && rc == PF_OK; ++it) {
+    float* o = (cur == L.p) ? L.p_alt : L.p;
+    rc = launch_sweep<float, float>(P, lv, cur, false, o, L.b, nullptr, V, nullptr, 1.f, reverse ? 1 : 0, false,
+                                    false, s);
+    cur = o;
+  }
+  P->prec = saved;
+  if (rc != PF_OK) return rc;
+  if (cur != L.p) PF_CUDA_TRY(cudaMemcpyAsync(L.p, cur, sizeof(float) * ncells(L), cudaMemcpyDeviceToDevice, s));
+  return PF_OK;
+}
+
+int pf_mg_solve(pf_mg_plan* P, const float* b, float* x, float tol, int32_t max_iter, int32_t use_graphs,
+                int32_t verbose, int32_t* iters_out, double* rel_out, void* stream) {
+  PF_REQUIRE(P && b && x && iters_out && rel_out, "null argument");
+  PF_REQUIRE(max_iter >= 0, "max_iter < 0");
+  cudaStream_t s = S(stream);
+  switch (P->prec) {
+    case PF_PREC_FP16: return solve_impl<__half>(P, b, x, tol, max_iter, use_graphs, verbose, iters_out, rel_out, s);
+    case PF_PREC_BF16:
+      return solve_impl<__nv_bfloat16>(P, b, x, tol, max_iter, use_graphs, verbose, iters_out, rel_out, s);
+    default: return solve_impl<float>(P, b, x, tol, max_iter, use_graphs, verbose, iters_out, rel_out, s);
+  }
+}
+
+int pf_apply_A(const pf_grid* g, const float* p, const float* bx, const float* by, const float* bz,
+               const float* diag, float* out, int32_t stencil, void* stream) {
+  PF_REQUIRE(g && p && bx && by && bz && out, "null argument");
+  PF_REQUIRE(stencil == PF_STENCIL_REFERENCE || stencil == PF_STENCIL_FLUX, "bad stencil");
+  const long long n = (long long)g->nx * g->ny * g->nz;
+  k_apply_A<<<ew_grid(n), 256, 0, S(stream)>>>(g->nx, g->ny, g->nz, p, bx, by, bz, diag, out,
+                                               stencil == PF_STENCIL_FLUX ? 1 : 0);
+  PF_LAUNCHED();
+  return PF_OK;
+}
+
+}  // extern "C"

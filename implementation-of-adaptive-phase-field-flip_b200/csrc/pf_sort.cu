@@ -1,0 +1,243 @@
+// Stable counting sort of particles by cell (no reference counterpart: the
+// reference keeps particles in seeding order, pfflip/scenes.py:23-29).
+//
+//   1. keys + histogram: key = linear index of the cell floor(x/dx) (IEEE
+//      binary32 division, clamped), counts by warp-aggregated atomics
+//   2. exclusive scan of the counts -> cell_start (3-phase block scan)
+//   3. scatter: slot = cursor[key]++ (warp-aggregated), perm[slot] = p
+//   4. per-cell order fix: atomics leave the slots of one cell in arrival
+//      order; one warp per cell ranks the original indices so each cell's
+//      segment is ascending, which is exactly a stable sort; sorted keys are
+//      written here
+//   5. gather of the two float4 particle streams through perm
+//
+// Bytes per particle: 16 (pos) + 4 (key) in pass 1, 8 in pass 3, 12 in pass 4,
+// 4 + 32 + 32 in pass 5, plus 8 per cell for the scan.
+#include "pf_common.cuh"
+
+namespace pf {
+
+__device__ __forceinline__ int cell_key(float x, float y, float z, float dx, int nx, int ny, int nz) {
+  int i = (int)floorf(x / dx), j = (int)floorf(y / dx), k = (int)floorf(z / dx);
+  i = min(max(i, 0), nx - 1);
+  j = min(max(j, 0), ny - 1);
+  k = min(max(k, 0), nz - 1);
+  return (i * ny + j) * nz + k;
+}
+
+// warp-aggregated atomicAdd(&ctr[key], 1): returns this lane's slot
+__device__ __forceinline__ int agg_inc(int* ctr, int key, unsigned active) {
+  const unsigned grp = __match_any_sync(active, key);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(grp) - 1;
+  const int rank = __popc(grp & ((1u << lane) - 1u));
+  int base = 0;
+  if (lane == leader) base = atomicAdd(ctr + key, __popc(grp));
+  base = __shfl_sync(grp, base, leader);
+  return base + rank;
+}
+
+__global__ void k_keys_hist(long long n, const float4* __restrict__ pos, float dx, int nx, int ny, int nz,
+                            int* __restrict__ keys, int* __restrict__ counts) {
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
+    const long long p = base + threadIdx.x;
+    const bool in = p < n;
+    const unsigned active = __ballot_sync(0xffffffffu, in);
+    if (!in) continue;
+    const float4 q = __ldg(pos + p);
+    const int key = cell_key(q.x, q.y, q.z, dx, nx, ny, nz);
+    keys[p] = key;
+    agg_inc(counts, key, active);
+  }
+}
+
+// ---------------------------------------------------------------- scan
+constexpr int SCAN_NT = 1024, SCAN_PER = 4, SCAN_TILE = SCAN_NT * SCAN_PER;
+
+__device__ __forceinline__ int block_excl_scan(int v, int* sh /*32*/, int* total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int s = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    sh[lane] = s;
+  }
+  __syncthreads();
+  const int before = (w > 0 ? sh[w - 1] : 0);
+  *total = sh[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return before + x - v;
+}
+
+// in place exclusive scan of a[0..n) per tile; tile totals to sums[]
+__global__ void __launch_bounds__(SCAN_NT) k_scan_tiles(long long n, int* __restrict__ a, int* __restrict__ sums) {
+  __shared__ int sh[32];
+  const long long t0 = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_PER;
+  int v[SCAN_PER], s = 0;
+#pragma unroll
+  for (int q = 0; q < SCAN_PER; ++q) {
+    v[q] = (t0 + q < n) ? a[t0 + q] : 0;
+    s += v[q];
+  }
+  int tot;
+  int ex = block_excl_scan(s, sh, &tot);
+#pragma unroll
+  for (int q = 0; q < SCAN_PER; ++q) {
+    if (t0 + q < n) a[t0 + q] = ex;
+    ex += v[q];
+  }
+  if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+// exclusive scan of the tile sums by one CTA (any count)
+__global__ void __launch_bounds__(SCAN_NT) k_scan_sums(int m, int* __restrict__ sums) {
+  __shared__ int sh[32];
+  int carry = 0;
+  for (int base = 0; base < m; base += SCAN_NT) {
+    const int i = base + threadIdx.x;
+    const int v = (i < m) ? sums[i] : 0;
+    int tot;
+    const int ex = block_excl_scan(v, sh, &tot);
+    if (i < m) sums[i] = carry + ex;
+    carry += tot;
+  }
+}
+
+__global__ void k_scan_add(long long n, int* __restrict__ a, const int* __restrict__ sums, int* __restrict__ cursor) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int v = a[e] + sums[e / SCAN_TILE];
+    a[e] = v;
+    if (cursor) cursor[e] = v;
+  }
+}
+
+// ---------------------------------------------------------------- scatter + order fix
+__global__ void k_scatter(long long n, const int* __restrict__ keys, int* __restrict__ cursor,
+                          int* __restrict__ perm) {
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
+    const long long p = base + threadIdx.x;
+    const bool in = p < n;
+    const unsigned active = __ballot_sync(0xffffffffu, in);
+    if (!in) continue;
+    const int key = keys[p];
+    const int slot = agg_inc(cursor, key, active);
+    perm[slot] = (int)p;
+  }
+}
+
+// one warp per cell: rank the segment's original indices (distinct) so the
+// segment becomes ascending; also writes the sorted keys
+__global__ void k_fix_order(int ncells, const int* __restrict__ start, int* __restrict__ perm,
+                            int* __restrict__ keys_out) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < ncells; c += warps) {
+    const int s = start[c], e = start[c + 1], len = e - s;
+    if (len == 0) continue;
+    for (int t = s + lane; t < e; t += 32) keys_out[t] = c;
+    if (len == 1) continue;
+    if (len <= 32) {
+      const int v = (lane < len) ? perm[s + lane] : INT_MAX;
+      // already ascending?  (the common case: arrivals were in order)
+      const int nxt = __shfl_down_sync(0xffffffffu, v, 1);
+      const bool ok = (lane >= len - 1) || (v < nxt);
+      if (__all_sync(0xffffffffu, ok)) continue;
+      int rank = 0;
+      for (int q = 0; q < len; ++q) rank += (__shfl_sync(0xffffffffu, v, q) < v);
+      __syncwarp();
+      if (lane < len) perm[s + rank] = v;
+    } else {
+      // long segment (> 32 particles in one cell): insertion sort by one lane.
+      // Arrivals are nearly ascending, so this is close to linear in practice.
+      if (lane == 0) {
+        for (int t = s + 1; t < e; ++t) {
+          const int v = perm[t];
+          int u = t - 1;
+          while (u >= s && perm[u] > v) {
+            perm[u + 1] = perm[u];
+            --u;
+          }
+          perm[u + 1] = v;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+__global__ void k_gather(long long n, const int* __restrict__ perm, const float4* __restrict__ pin,
+                         const float4* __restrict__ vin, float4* __restrict__ pout, float4* __restrict__ vout) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int p = perm[t];
+    pout[t] = __ldg(pin + p);
+    vout[t] = __ldg(vin + p);
+  }
+}
+
+}  // namespace pf
+
+using namespace pf;
+
+extern "C" {
+
+size_t pf_sort_workspace_bytes(const pf_grid* g, int64_t n) {
+  if (!g) return 0;
+  const long long nc = (long long)g->nx * g->ny * g->nz;
+  const long long tiles = (nc + 1 + SCAN_TILE - 1) / SCAN_TILE;
+  return (size_t)(4 * n + 4 * (nc + 1) + 4 * (tiles + 1) + 256);
+}
+
+int pf_sort_particles(const pf_grid* g, int64_t n, const float* pos4_in, const float* vel4_in, float* pos4_out,
+                      float* vel4_out, int32_t* keys_out, int32_t* perm_out, int32_t* cell_start, void* workspace,
+                      size_t workspace_bytes, void* stream) {
+  PF_REQUIRE(g && n >= 0 && pos4_in && vel4_in && pos4_out && vel4_out && keys_out && perm_out && cell_start,
+             "null argument");
+  PF_REQUIRE(g->nx > 0 && g->ny > 0 && g->nz > 0 && g->dx > 0.f, "bad grid");
+  PF_REQUIRE((long long)g->nx * g->ny * g->nz < (1LL << 31) && n < (1LL << 31), "too large for int32 indices");
+  PF_REQUIRE(aligned16(pos4_in) && aligned16(vel4_in) && aligned16(pos4_out) && aligned16(vel4_out),
+             "particle streams must be 16-byte aligned");
+  PF_REQUIRE(pos4_in != pos4_out && vel4_in != vel4_out, "sort output must not alias its input");
+  PF_REQUIRE(workspace && workspace_bytes >= pf_sort_workspace_bytes(g, n), "workspace too small");
+  cudaStream_t s = S(stream);
+  const long long nc = (long long)g->nx * g->ny * g->nz;
+  const long long tiles = (nc + 1 + SCAN_TILE - 1) / SCAN_TILE;
+  int* keys_tmp = reinterpret_cast<int*>(workspace);
+  int* cursor = keys_tmp + n;
+  int* sums = cursor + (nc + 1);
+  PF_CUDA_TRY(cudaMemsetAsync(cell_start, 0, sizeof(int) * (nc + 1), s));
+  if (n > 0) {
+    k_keys_hist<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, reinterpret_cast<const float4*>(pos4_in), g->dx,
+                                                               g->nx, g->ny, g->nz, keys_tmp, cell_start);
+    PF_LAUNCHED();
+  }
+  k_scan_tiles<<<(int)tiles, SCAN_NT, 0, s>>>(nc + 1, cell_start, sums);
+  PF_LAUNCHED();
+  k_scan_sums<<<1, SCAN_NT, 0, s>>>((int)tiles, sums);
+  PF_LAUNCHED();
+  k_scan_add<<<grid_for(nc + 1, 256, kNumSMs * 16), 256, 0, s>>>(nc + 1, cell_start, sums, cursor);
+  PF_LAUNCHED();
+  if (n == 0) return PF_OK;
+  k_scatter<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, keys_tmp, cursor, perm_out);
+  PF_LAUNCHED();
+  k_fix_order<<<grid_for(nc * 32, 256, kNumSMs * 16), 256, 0, s>>>((int)nc, cell_start, perm_out, keys_out);
+  PF_LAUNCHED();
+  k_gather<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, perm_out, reinterpret_cast<const float4*>(pos4_in),
+                                                          reinterpret_cast<const float4*>(vel4_in),
+                                                          reinterpret_cast<float4*>(pos4_out),
+                                                          reinterpret_cast<float4*>(vel4_out));
+  PF_LAUNCHED();
+  return PF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,361 @@
+"""PF-FLIP simulator on a uniform MAC grid (B200, sm_100a).
+
+``Simulator`` keeps the constructor, methods, stage methods, attributes and
+stats of the reference's ``pfflip.sim.Simulator`` (``pfflip/sim.py:37-424``) for
+the uniform step; all stage work runs in libpfflip.so:
+
+==========================  ===============================================
+reference stage              libpfflip entry point(s)
+==========================  ===============================================
+(new) particle sort          pf_sort_particles
+``_p2g``                     pf_p2g (+ the face velocities in pf_phase_beta)
+``_phase_field_and_coef.``   pf_phase_beta
+vel_star copy + forces       pf_save_and_force
+``_pressure_solve``          pf_build_rhs, pf_mg_build_hierarchy, pf_mg_solve
+``_project``                 pf_project
+``_max_divergence``          pf_max_divergence
+``_extrapolate_liquid_vel.`` pf_extrapolate
+``_g2p`` + ``_advect``       pf_g2p_advect (one fused pass inside ``step``)
+==========================  ===============================================
+
+Particles live on the device as two float4 streams sorted by cell (see
+include/pfflip.h); ``px``, ``pv``, ``ptype``, ``pmass``, ``pstate`` present them
+in the caller's original order.  The droplet stage (``cfg.droplets``) is not
+part of this implementation and is skipped with a warning.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+import warnings
+
+import numpy as np
+import torch
+
+from . import _native as N
+from ._arrays import DeviceArray, as_tensor
+from .config import Config
+from .poisson import MGPCG, default_coef_scale
+
+
+def calibrate_rho_tilde_0(dx: float, r: float, ppc: int) -> float:
+    """rho~_0: eq. (6) kernel-weight sum at a point of a perfect lattice.
+
+    The lattice has ``round(ppc^(1/3))`` sites per cell and axis; the sample
+    point sits half a lattice step off every site, as in the reference's
+    calibration (pfflip/sim.py:119-140)."""
+    pa = round(ppc ** (1.0 / 3.0))
+    step = dx / pa
+    R = int(math.ceil(r / step)) + 1
+    o2 = (np.arange(-R, R + 1) + 0.5) ** 2
+    d2 = (o2[:, None, None] + o2[None, :, None] + o2[None, None, :]) * step * step
+    t = np.maximum(1.0 - d2 / (r * r), 0.0)
+    return float((t * t * t).sum())
+
+
+class ParticleField:
+    """One particle attribute in the caller's original order.
+
+    ``numpy()`` un-permutes the sorted device streams; ``assign(a)`` writes an
+    array given in original order into the sorted slots."""
+
+    def __init__(self, sim, kind):
+        self._sim = sim
+        self._kind = kind
+
+    @property
+    def shape(self):
+        n = self._sim.n_particles
+        return (n, 3) if self._kind in ("pos", "vel") else (n,)
+
+    def _tensor(self):
+        s, k = self._sim, self._kind
+        ids = s._ids().long()
+        if k in ("pos", "vel"):
+            src = (s._pos4 if k == "pos" else s._vel4)[:, :3]
+            out = torch.empty_like(src)
+            out[ids] = src
+            return out
+        flags = s._flags()
+        if k == "ptype":
+            v = flags & N_FLAG_LIQUID
+        elif k == "pstate":
+            v = (flags >> N_PSTATE_SHIFT) & 3
+        elif k == "pmass":
+            cfg = s.cfg
+            v = torch.where((flags & N_FLAG_LIQUID) != 0, torch.tensor(cfg.rho_l, dtype=torch.float32, device=s.dev),
+                            torch.tensor(cfg.rho_g, dtype=torch.float32, device=s.dev))
+        elif k == "prad":
+            v = torch.full_like(flags, 0, dtype=torch.float32) + float(np.float32(s.cfg.r_p))
+        out = torch.empty_like(v)
+        out[ids] = v
+        return out
+
+    def numpy(self):
+        return self._tensor().cpu().numpy()
+
+    def __array__(self, dtype=None, copy=None):
+        a = self.numpy()
+        return a if dtype is None else a.astype(dtype)
+
+    def assign(self, a):
+        s, k = self._sim, self._kind
+        ids = s._ids().long()
+        t = torch.as_tensor(np.ascontiguousarray(np.asarray(a))).to(s.dev)
+        if k in ("pos", "vel"):
+            dst = s._pos4 if k == "pos" else s._vel4
+            dst[:, :3] = t.reshape(-1, 3).to(torch.float32)[ids]
+            return self
+        if k not in ("ptype", "pstate"):
+            raise TypeError(f"{k} is derived from the particle type and cannot be assigned")
+        flags = s._flags()
+        v = t.reshape(-1).to(torch.int32)[ids]
+        if k == "ptype":
+            flags = (flags & ~N_FLAG_LIQUID) | (v == 1).to(torch.int32)
+        else:
+            flags = (flags & N_FLAG_LIQUID) | ((v & 3) << N_PSTATE_SHIFT)
+        s._pos4.view(torch.int32)[:, 3] = flags
+        return self
+
+
+N_FLAG_LIQUID = 1
+N_PSTATE_SHIFT = 1
+
+
+class Simulator:
+    def __init__(self, cfg: Config):
+        self.cfg = cfg
+        self.dev = N.require_cuda(cfg.device)
+        nx, ny, nz = (int(n) for n in cfg.res)
+        self.res = (nx, ny, nz)
+        self._g = N.grid(self.res, np.float32(cfg.dx))
+        self.face_shapes = ((nx + 1, ny, nz), (nx, ny + 1, nz), (nx, ny, nz + 1))
+        z = lambda shape: DeviceArray.zeros(shape, torch.float32, self.dev)  # noqa: E731
+        zi = lambda shape: DeviceArray.zeros(shape, torch.int32, self.dev)  # noqa: E731
+        fs = self.face_shapes
+        self.vel = [z(s) for s in fs]
+        self.vel_star = [z(s) for s in fs]
+        self.vel_liq = [z(s) for s in fs]
+        self.mass = [z(s) for s in fs]
+        self.mom = [z(s) for s in fs]
+        self.beta = [z(s) for s in fs]
+        self.phi_face = [z(s) for s in fs]
+        self.valid = [zi(s) for s in fs]
+        self._known = [zi(s) for s in fs]
+        self.cell_mass = z(self.res)
+        self.cell_wsum = z(self.res)
+        self.phi_cell = z(self.res)
+        self.is_liquid = zi(self.res)
+        self.solid = zi(self.res)
+        self.pressure = z(self.res)
+        self.rhs = z(self.res)
+        self._scal = torch.zeros(8, dtype=torch.float32, device=self.dev)
+
+        self.solver = MGPCG(
+            self.res, self.dev, omega=cfg.mg_omega, pre=cfg.mg_pre_sweeps, post=cfg.mg_post_sweeps,
+            coarsest=cfg.mg_coarsest_sweeps, min_dim=cfg.mg_min_dim, precision=cfg.precision,
+            stencil=cfg.stencil, coef_scale=default_coef_scale(cfg.rho_l, cfg.rho_g), use_graphs=cfg.cuda_graphs,
+        )
+
+        self.n_particles = 0
+        self._pos4 = self._vel4 = None
+        self.droplet_stats = {"emitted": 0, "bubbles": 0, "merged": 0, "spray": 0}
+
+        self.rho_tilde_0 = calibrate_rho_tilde_0(cfg.dx, cfg.r_p, cfg.ppc)
+        self.rho_0l = self.rho_tilde_0 * cfg.rho_l
+        self.rho_min = cfg.eta_phi * cfg.rho_g * self.rho_tilde_0
+
+        self.has_solids = False
+        self.time = 0.0
+        self.step_index = 0
+        self.stats: list[dict] = []
+        self._warned_droplets = False
+
+        self.px = ParticleField(self, "pos")
+        self.pv = ParticleField(self, "vel")
+        self.ptype = ParticleField(self, "ptype")
+        self.pstate = ParticleField(self, "pstate")
+        self.pmass = ParticleField(self, "pmass")
+        self.prad = ParticleField(self, "prad")
+
+    # ------------------------------------------------------------------ setup
+    def set_solids(self, mask: np.ndarray):
+        """Install an obstacle mask (True = solid) on the cell grid."""
+        self.solid.assign(np.ascontiguousarray(mask, np.int32))
+        self.has_solids = bool(np.any(mask))
+
+    def set_particles(self, pos: np.ndarray, vel: np.ndarray, ptype: np.ndarray):
+        """Upload particles (NumPy (n,3) positions and velocities, (n,) types)."""
+        pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        vel = np.ascontiguousarray(vel, np.float32).reshape(-1, 3)
+        ptype = np.ascontiguousarray(ptype).reshape(-1)
+        n = len(pos)
+        if len(vel) != n or len(ptype) != n:
+            raise ValueError("pos, vel and ptype must have the same length")
+        self.n_particles = n
+        dev = self.dev
+        p4 = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        v4 = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        p4[:, :3] = torch.from_numpy(pos).to(dev)
+        v4[:, :3] = torch.from_numpy(vel).to(dev)
+        p4.view(torch.int32)[:, 3] = torch.from_numpy((ptype == 1).astype(np.int32)).to(dev)
+        v4.view(torch.int32)[:, 3] = torch.arange(n, dtype=torch.int32, device=dev)
+        self._pos4, self._vel4 = p4, v4
+        self._pos4_alt = torch.empty_like(p4)
+        self._vel4_alt = torch.empty_like(v4)
+        self._keys = torch.empty(n, dtype=torch.int32, device=dev)
+        self._perm = torch.empty(n, dtype=torch.int32, device=dev)
+        nc = self.res[0] * self.res[1] * self.res[2]
+        self._cell_start = torch.zeros(nc + 1, dtype=torch.int32, device=dev)
+        wsb = int(N.lib().pf_sort_workspace_bytes(C.byref(self._g), n))
+        self._sort_ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+        self._sort()
+
+    def _ids(self):
+        return self._vel4.view(torch.int32)[:, 3]
+
+    def _flags(self):
+        return self._pos4.view(torch.int32)[:, 3]
+
+    def _sort(self):
+        """Counting sort of the particle streams by cell (new stage; the
+        reference never reorders particles)."""
+        n = self.n_particles
+        N.call("pf_sort_particles", C.byref(self._g), n, self._pos4.data_ptr(), self._vel4.data_ptr(),
+               self._pos4_alt.data_ptr(), self._vel4_alt.data_ptr(), self._keys.data_ptr(), self._perm.data_ptr(),
+               self._cell_start.data_ptr(), self._sort_ws.data_ptr(), self._sort_ws.numel(), N.stream())
+        self._pos4, self._pos4_alt = self._pos4_alt, self._pos4
+        self._vel4, self._vel4_alt = self._vel4_alt, self._vel4
+
+    # ------------------------------------------------------------------ step
+    def dt_from_cfl(self) -> float:
+        cfg = self.cfg
+        N.call("pf_particle_max_speed", self.n_particles, self._pos4.data_ptr(), self._vel4.data_ptr(),
+               self._scal.data_ptr(), N.stream())
+        vmax = float(self._scal[0].item())
+        g = float(np.linalg.norm(cfg.gravity))
+        vmax = max(vmax, math.sqrt(2.0 * g * cfg.dx) if g > 0 else 0.0, 1e-8)
+        return float(np.clip(cfg.cfl * cfg.dx / vmax, cfg.dt_min, cfg.dt_max))
+
+    def step(self, dt: float | None = None, verbose: bool = False) -> dict:
+        if dt is None:
+            dt = self.dt_from_cfl()
+        t0 = time.perf_counter()
+        self._p2g()
+        self._phase_field_and_coefficients()
+        self._add_forces(dt, save_vel_star=True)
+        pcg_it, pcg_res = self._pressure_solve(dt, verbose=verbose)
+        self._project(dt)
+        self._divergence_async()
+        self._extrapolate_liquid_velocity()
+        self._droplets(dt)
+        self._g2p_advect(dt, do_g2p=True, do_advect=True)
+        div_after = float(self._scal[1].item())  # synchronises the stream
+        wall = time.perf_counter() - t0
+        self.time += dt
+        self.step_index += 1
+        rec = {
+            "step": self.step_index,
+            "t": self.time,
+            "dt": dt,
+            "pcg_iter": pcg_it,
+            "pcg_res": pcg_res,
+            "max_div": div_after,
+            "droplets": 0,
+            "wall_s": wall,
+        }
+        self.stats.append(rec)
+        return rec
+
+    # ------------------------------------------------------------------ stages
+    def _p2g(self):
+        """Sort, then eq. (3)-(6) splatting to faces and cells (pfflip/sim.py:205-236)."""
+        cfg = self.cfg
+        self._sort()
+        N.call("pf_p2g", C.byref(self._g), self.n_particles, self._pos4.data_ptr(), self._vel4.data_ptr(),
+               self._cell_start.data_ptr(), float(cfg.rho_l), float(cfg.rho_g), float(np.float32(cfg.r_p)),
+               *(N.ptr(a) for a in self.mass), *(N.ptr(a) for a in self.mom), N.ptr(self.cell_mass),
+               N.ptr(self.cell_wsum), N.stream())
+
+    def _phase_field_and_coefficients(self):
+        """u = P/m, eq. (7) phi, eq. (9) beta, walls and obstacles (pfflip/sim.py:229-268)."""
+        cfg = self.cfg
+        N.call("pf_phase_beta", C.byref(self._g), *(N.ptr(a) for a in self.mass), *(N.ptr(a) for a in self.mom),
+               N.ptr(self.cell_mass), N.ptr(self.solid) if self.has_solids else None, float(1e-12 * self.rho_0l),
+               float(self.rho_min), float(cfg.alpha_phi), float(self.rho_0l), float(cfg.rho_l), float(cfg.rho_g),
+               *(N.ptr(a) for a in self.vel), *(N.ptr(a) for a in self.valid), N.ptr(self.phi_cell),
+               N.ptr(self.is_liquid), *(N.ptr(a) for a in self.phi_face), *(N.ptr(a) for a in self.beta), N.stream())
+
+    def _add_forces(self, dt: float, save_vel_star: bool = False):
+        """Gravity and wall/obstacle zeroing (pfflip/sim.py:270-285); with
+        save_vel_star the pre-force copy of pfflip/sim.py:176-177 is fused in."""
+        g = self.cfg.gravity
+        vs = [N.ptr(a) for a in self.vel_star] if save_vel_star else [None, None, None]
+        N.call("pf_save_and_force", C.byref(self._g), *(N.ptr(a) for a in self.vel), *vs,
+               N.ptr(self.solid) if self.has_solids else None, float(g[0]), float(g[1]), float(g[2]), float(dt),
+               N.stream())
+
+    def _pressure_solve(self, dt: float, verbose: bool = False):
+        cfg = self.cfg
+        N.call("pf_build_rhs", C.byref(self._g), *(N.ptr(a) for a in self.vel), N.ptr(self.cell_wsum),
+               N.ptr(self.rhs), float(dt), float(self.rho_tilde_0), float(cfg.k_div), N.stream())
+        self.solver.build_hierarchy(*self.beta)
+        return self.solver.solve(self.rhs, self.pressure, tol=cfg.pcg_tol, max_iter=cfg.pcg_max_iter,
+                                 verbose=verbose)
+
+    def _project(self, dt: float):
+        N.call("pf_project", C.byref(self._g), N.ptr(self.pressure), *(N.ptr(a) for a in self.beta),
+               *(N.ptr(a) for a in self.vel), float(dt), N.stream())
+
+    def _divergence_async(self):
+        N.call("pf_max_divergence", C.byref(self._g), *(N.ptr(a) for a in self.vel), self._scal.data_ptr() + 4,
+               N.stream())
+
+    def _max_divergence(self) -> float:
+        self._divergence_async()
+        return float(self._scal[1].item())
+
+    def _extrapolate_liquid_velocity(self):
+        N.call("pf_extrapolate", C.byref(self._g), *(N.ptr(a) for a in self.vel), N.ptr(self.is_liquid),
+               int(self.cfg.extrap_cells), *(N.ptr(a) for a in self.vel_liq), *(N.ptr(a) for a in self._known),
+               N.stream())
+
+    def _bounds(self):
+        eps = 1e-4 * self.cfg.dx
+        lo = (C.c_float * 3)(eps, eps, eps)
+        hi = (C.c_float * 3)(*[s - eps for s in self.cfg.domain_size])
+        return lo, hi
+
+    def _g2p_advect(self, dt, do_g2p, do_advect):
+        lo, hi = self._bounds()
+        cfg = self.cfg
+        N.call("pf_g2p_advect", C.byref(self._g), self.n_particles, self._pos4.data_ptr(), self._vel4.data_ptr(),
+               *(N.ptr(a) for a in self.vel), *(N.ptr(a) for a in self.vel_star), *(N.ptr(a) for a in self.vel_liq),
+               N.ptr(self.solid) if self.has_solids else None, float(cfg.alpha_flip_liquid),
+               float(cfg.alpha_flip_air), float(dt), lo, hi, int(do_g2p), int(do_advect), N.stream())
+
+    def _g2p(self):
+        """eq. (11)-(12) FLIP/PIC update (pfflip/sim.py:316-327)."""
+        self._g2p_advect(0.0, do_g2p=True, do_advect=False)
+
+    def _advect(self, dt: float):
+        """RK3 advection and wall reflection (pfflip/sim.py:408-424); needs
+        ``_extrapolate_liquid_velocity`` first, as in the reference."""
+        self._g2p_advect(dt, do_g2p=False, do_advect=True)
+
+    def _droplets(self, dt: float):
+        if self.cfg.droplets and not self._warned_droplets:
+            warnings.warn("the droplet/spray stage is not part of this implementation; cfg.droplets is ignored",
+                          RuntimeWarning, stacklevel=3)
+            self._warned_droplets = True
+
+    @property
+    def dvel(self):
+        """u - u* per axis (the reference's FLIP difference field)."""
+        return [DeviceArray(as_tensor(a) - as_tensor(b)) for a, b in zip(self.vel, self.vel_star)]
+
+    def state_counts(self):
+        st = self.pstate.numpy()
+        return {"flip": int((st == 0).sum()), "droplet": int((st == 1).sum()), "dead": int((st == 2).sum())}

@@ -1,0 +1,208 @@
+"""The reference's end-to-end property tests (tests/test_pfflip.py) run against
+the drop-in Simulator on the GPU.
+
+Same scenes, sizes, step counts and thresholds as the reference file
+(line numbers in each docstring).  The droplet stage is outside this
+implementation, so configurations set ``droplets=False`` and the two
+droplet-transition tests of the reference (:124-137, :140-167 asserts on
+droplet conversion) are not ported; the ones that only use ``pstate``
+(:170-189, :245-268) are.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+from pfflip import Config, Simulator, copy, scenes
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+
+
+@pytest.fixture(scope="module")
+def pool():
+    cfg = Config(res=(32, 32, 32), dx=1.0 / 32, cfl=1.0, device=DEV, droplets=False)
+    sim = Simulator(cfg)
+    sim.set_particles(*scenes.still_pool(cfg, fill=0.5))
+    return sim
+
+
+def test_rho_tilde_0_matches_closed_form():
+    """tests/test_pfflip.py:35-41"""
+    cfg = Config(res=(8, 8, 8), dx=1.0 / 8, device=DEV, droplets=False)
+    sim = Simulator(cfg)
+    n_p = cfg.ppc / cfg.dx**3
+    analytic = n_p * 64.0 * np.pi * cfg.r_p**3 / 315.0
+    assert abs(sim.rho_tilde_0 - analytic) / analytic < 0.05
+
+
+def test_phase_field_saturates(pool):
+    """tests/test_pfflip.py:44-62"""
+    pool.step()
+    phi = pool.phi_cell.numpy()
+    ny = phi.shape[1]
+    air = phi[:, 3 * ny // 4:, :]
+    liq = phi[:, : ny // 4, :]
+    assert air.max() == 0.0, f"air phase is not clean: max phi = {air.max()}"
+    assert liq.mean() > 0.95, f"liquid bulk not saturated on average: {liq.mean()}"
+    assert liq.min() > 0.6, f"noise reaches the 0.5 tag threshold: min phi = {liq.min()}"
+
+
+def test_interface_thickness_one_cell(pool):
+    """tests/test_pfflip.py:65-74"""
+    pool.step()
+    phi = pool.phi_cell.numpy()
+    col = phi[16, :, 16]
+    inside = np.where(col > 0.95)[0]
+    outside = np.where(col < 0.05)[0]
+    gap = outside[outside > inside.max()].min() - inside.max()
+    assert gap <= 3, f"interface spans {gap} cells; eps_phi should be ~1 cell"
+
+
+def test_mass_conserved_exactly():
+    """tests/test_pfflip.py:77-87"""
+    cfg = Config(res=(24, 24, 24), dx=1.0 / 24, cfl=1.0, device=DEV, droplets=False)
+    sim = Simulator(cfg)
+    sim.set_particles(*scenes.dam_break(cfg))
+    m0 = sim.pmass.numpy().sum()
+    n0 = (sim.ptype.numpy() == 1).sum()
+    for _ in range(10):
+        sim.step()
+    assert sim.pmass.numpy().sum() == m0
+    assert (sim.ptype.numpy() == 1).sum() == n0
+
+
+def test_hydrostatic_equilibrium_is_stable(pool):
+    """tests/test_pfflip.py:90-103"""
+    liq = pool.ptype.numpy() == 1
+    y0 = pool.px.numpy()[liq, 1].mean()
+    speeds = []
+    for _ in range(30):
+        pool.step()
+        speeds.append(np.linalg.norm(pool.pv.numpy()[liq], axis=1).max())
+    y1 = pool.px.numpy()[liq, 1].mean()
+    g_dt = 9.81 * pool.stats[-1]["dt"]
+    assert max(speeds) < 0.5 * g_dt, f"spurious liquid motion {max(speeds):.3f} vs g*dt {g_dt:.3f}"
+    assert abs(y1 - y0) < 0.01 * pool.cfg.domain_size[1], "liquid centroid drifted"
+    assert speeds[-1] <= speeds[0] * 1.5, "velocities are growing, not decaying"
+
+
+@pytest.mark.parametrize("stencil", ["flux", "reference"])
+def test_projection_reduces_divergence(stencil):
+    """tests/test_pfflip.py:106-120"""
+    cfg = Config(res=(32, 32, 32), dx=1.0 / 32, cfl=1.0, device=DEV, pcg_tol=1e-5, droplets=False,
+                 stencil=stencil)
+    sim = Simulator(cfg)
+    sim.set_particles(*scenes.dam_break(cfg))
+    sim._p2g()
+    sim._phase_field_and_coefficients()
+    for ax in range(3):
+        copy(sim.vel_star[ax], sim.vel[ax])
+    dt = 1e-3
+    sim._add_forces(dt)
+    div_before = sim._max_divergence()
+    sim._pressure_solve(dt)
+    sim._project(dt)
+    div_after = sim._max_divergence()
+    assert div_after < 0.05 * div_before, f"{div_before:.3e} -> {div_after:.3e}"
+
+
+def test_droplet_threshold_is_coupled_to_particle_count():
+    """tests/test_pfflip.py:140-167, its rho~_0 part (no droplet stage here)."""
+    for ppc in (8, 27):
+        cfg = Config(res=(16,) * 3, dx=1 / 16, device=DEV, ppc=ppc, droplets=False)
+        sim = Simulator(cfg)
+        phi_single = 1.0 / math.sqrt(cfg.alpha_phi * sim.rho_tilde_0)
+        predicted = 0.638 * ppc
+        assert abs(sim.rho_tilde_0 - predicted) / predicted < 0.10
+        assert (phi_single < 0.5 - cfg.delta_phi) == (ppc >= 18)
+
+
+def test_droplets_do_not_contribute_to_the_grid():
+    """tests/test_pfflip.py:170-189: particles with pstate != 0 do not splat."""
+    cfg = Config(res=(16,) * 3, dx=1 / 16, cfl=1.0, device=DEV, ppc=8, droplets=False)
+    sim = Simulator(cfg)
+    sim.set_particles(*scenes.still_pool(cfg, fill=0.5))
+    sim.step()
+    m_all = sim.cell_mass.numpy().sum()
+    st = sim.pstate.numpy()
+    liq = np.flatnonzero(sim.ptype.numpy() == 1)
+    st[liq[::10]] = 1
+    sim.pstate.assign(st)
+    sim._p2g()
+    m_flip = sim.cell_mass.numpy().sum()
+    assert m_flip < m_all
+    removed = 1.0 - m_flip / m_all
+    assert abs(removed - 0.10) < 0.02, f"expected ~10% of mass removed, got {100 * removed:.1f}%"
+
+
+def test_obstacle_does_not_leak_gravity():
+    """tests/test_pfflip.py:193-222"""
+    cfg = Config(res=(32,) * 3, dx=1 / 32, cfl=1.0, device=DEV, ppc=8, droplets=False)
+    sim = Simulator(cfg)
+    pos, vel, pt, solid = scenes.wave_vs_tower(cfg)
+    sim.set_particles(pos, vel, pt)
+    sim.set_solids(solid)
+    assert solid.sum() > 0
+    for _ in range(5):
+        sim.step()
+    for ax in range(3):
+        beta = sim.beta[ax].numpy()
+        v = sim.vel[ax].numpy()
+        blocked = beta == 0.0
+        assert blocked.any()
+        assert np.abs(v[blocked]).max() == 0.0
+
+
+def test_obstacle_scene_stays_bounded():
+    """tests/test_pfflip.py:225-242"""
+    cfg = Config(res=(32,) * 3, dx=1 / 32, cfl=1.0, device=DEV, ppc=8, droplets=False)
+    sim = Simulator(cfg)
+    pos, vel, pt, solid = scenes.wave_vs_tower(cfg)
+    sim.set_particles(pos, vel, pt)
+    sim.set_solids(solid)
+    v0 = float(np.abs(sim.pv.numpy()).max())
+    speeds = []
+    for _ in range(40):
+        sim.step()
+        st = sim.pstate.numpy()
+        speeds.append(float(np.linalg.norm(sim.pv.numpy()[st == 0], axis=1).max()))
+    assert max(speeds) < 12 * v0, f"|v| reached {max(speeds):.1f} from v0 = {v0:.2f}"
+    assert np.isfinite(speeds).all()
+
+
+def test_droplets_do_not_throttle_the_time_step():
+    """tests/test_pfflip.py:245-268"""
+    cfg = Config(res=(32,) * 3, dx=1 / 32, cfl=1.0, device=DEV, ppc=8, droplets=False)
+    sim = Simulator(cfg)
+    sim.set_particles(*scenes.asteroid_impact(cfg))
+    sim.step()
+    v = sim.pv.numpy()
+    st = sim.pstate.numpy()
+    v[0] = (500.0, 0.0, 0.0)
+    st[0] = 1
+    v[1] = (500.0, 0.0, 0.0)
+    st[1] = 2
+    sim.pv.assign(v)
+    sim.pstate.assign(st)
+    dt = sim.dt_from_cfl()
+    assert dt > cfg.dx / 50.0, f"a single fast droplet collapsed dt to {dt:.2e}"
+
+
+def test_particle_views_round_trip():
+    """px/pv/ptype/pstate present the caller's original order across sorts."""
+    cfg = Config(res=(16,) * 3, dx=1 / 16, ppc=8, droplets=False)
+    sim = Simulator(cfg)
+    pos, vel, pt = scenes.dam_break(cfg)
+    rng = np.random.default_rng(0)
+    vel = rng.standard_normal(pos.shape).astype(np.float32)
+    sim.set_particles(pos, vel, pt)
+    assert np.array_equal(sim.px.numpy(), pos) and np.array_equal(sim.pv.numpy(), vel)
+    assert np.array_equal(sim.ptype.numpy(), pt)
+    pos2 = pos[::-1].copy()
+    sim.px.assign(pos2)
+    sim._sort()
+    assert np.array_equal(sim.px.numpy(), pos2) and np.array_equal(sim.pv.numpy(), vel)
+    assert sim.pmass.numpy().dtype == np.float32
+    assert sim.state_counts() == {"flip": len(pos), "droplet": 0, "dead": 0}

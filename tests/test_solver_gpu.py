@@ -1,0 +1,196 @@
+"""GPU parity of the Poisson solver (libpfflip.so) against the reference's
+test vectors and the CPU oracle.
+
+Mirrors tests/test_poisson.py of the reference (operator vs assembled matrix,
+MG-PCG vs spsolve at contrast 1 and 1000) through the drop-in API, then pins
+each solver stage against the oracle (oracle/pf_oracle.hpp).
+
+Tolerances: hierarchy coefficients are sums in the reference's order, so they
+must match bit for bit; smoother and V-cycle outputs differ from the oracle
+only by FMA contraction (<= 1e-5 relative to the field's max); solves agree
+within the solver tolerance.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from pfflip import launch, scenes
+from pfflip._arrays import DeviceArray
+from pfflip.poisson import MGPCG, apply_A
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+RES = (16, 16, 16)
+
+
+def dev(a, dtype=torch.float32):
+    return DeviceArray(torch.as_tensor(np.ascontiguousarray(a)).to(DEV, dtype))
+
+
+def rel_err(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+@pytest.mark.parametrize("contrast", [1.0, 1000.0])
+@pytest.mark.parametrize("stencil", ["reference", "flux"])
+def test_operator_matches_assembled(golden, contrast, stencil):
+    arrays, _ = golden
+    tag = f"c{int(contrast)}"
+    bx, by, bz = (arrays[f"op_{tag}_{n}"] for n in ("bx", "by", "bz"))
+    p, ref = arrays[f"op_{tag}_p"], arrays[f"op_{tag}_Ap"]
+    solver = MGPCG(RES, DEV)
+    solver.build_hierarchy(dev(bx), dev(by), dev(bz))
+    out = DeviceArray.zeros(RES, device=DEV)
+    L0 = solver.levels[0]
+    if stencil == "reference":
+        launch(apply_A, dim=RES, inputs=[dev(p), L0.bx, L0.by, L0.bz, L0.diag, out], device=DEV)
+    else:
+        apply_A(dev(p), L0.bx, L0.by, L0.bz, None, out, stencil="flux")
+    got = out.numpy()
+    assert np.abs(got - ref).max() < 1e-3 * max(1.0, np.abs(ref).max())
+    # and against the oracle's binary32 operator of the same form: FMA contraction only
+    assert rel_err(got, O.apply_A(p, bx, by, bz, O.compute_diag(bx, by, bz), stencil=stencil)) < 1e-6
+
+
+@pytest.mark.parametrize("contrast", [1.0, 1000.0])
+@pytest.mark.parametrize("graphs,stencil", [(True, "flux"), (False, "flux"), (True, "reference")])
+def test_mgpcg_solves(golden, contrast, graphs, stencil):
+    arrays, _ = golden
+    tag = f"c{int(contrast)}"
+    bx, by, bz, b, ref = (arrays[f"solve_{tag}_{n}"] for n in ("bx", "by", "bz", "b", "x"))
+    solver = MGPCG(RES, DEV, use_graphs=graphs, stencil=stencil)
+    solver.build_hierarchy(dev(bx), dev(by), dev(bz))
+    pw = DeviceArray.zeros(RES, device=DEV)
+    it, rel = solver.solve(dev(b), pw, tol=1e-5, max_iter=400)
+    assert rel < 1e-5, f"MG-PCG stalled at {rel:.2e} after {it} iterations"
+    got = pw.numpy().astype(np.float64).ravel()
+    got -= got.mean()
+    err = np.abs(got - ref.ravel()).max() / np.abs(ref).max()
+    assert err < 1e-3
+
+
+def test_hierarchy_matches_oracle_bitwise():
+    bx, by, bz, b, _ = scenes.solve_problem((32, 32, 32), seed=3)
+    g = MGPCG((32,) * 3, DEV, pre=3, post=3)
+    g.build_hierarchy(dev(bx), dev(by), dev(bz))
+    o = O.OracleMGPCG((32,) * 3, pre=3, post=3)
+    o.build_hierarchy(bx, by, bz)
+    assert g.nlev == o.nlev == 4
+    for lv, L in enumerate(g.levels):
+        for name in ("bx", "by", "bz", "diag"):
+            assert np.array_equal(getattr(L, name).numpy(), o.level_array(lv, name)), (lv, name)
+
+
+@pytest.mark.parametrize("stencil", ["reference", "flux"])
+def test_smoother_matches_oracle(stencil):
+    rng = np.random.default_rng(5)
+    res = (24, 40, 36)  # not multiples of the tile, odd level count
+    bx, by, bz, _, _ = scenes.solve_problem(res, seed=4)
+    g = MGPCG(res, DEV, stencil=stencil)
+    g.build_hierarchy(dev(bx), dev(by), dev(bz))
+    o = O.OracleMGPCG(res, stencil=stencil)
+    o.build_hierarchy(bx, by, bz)
+    p0 = rng.standard_normal(res).astype(np.float32)
+    b0 = rng.standard_normal(res).astype(np.float32)
+    for reverse in (False, True):
+        g.levels[0].p.assign(p0)
+        g.levels[0].b.assign(b0)
+        o.set_level_array(0, "p", p0)
+        o.set_level_array(0, "b", b0)
+        for nsw in (1, 2, 3):
+            g._smooth(g.levels[0], nsw, reverse=reverse)
+            o.smooth(0, nsw, reverse=reverse)
+            assert rel_err(g.levels[0].p.numpy(), o.level_array(0, "p")) < 1e-5, (reverse, nsw)
+
+
+@pytest.mark.parametrize("res", [(32, 32, 32), (16, 24, 40), (20, 20, 20)])
+@pytest.mark.parametrize("stencil", ["reference", "flux"])
+def test_precondition_matches_oracle(res, stencil):
+    bx, by, bz, b, _ = scenes.solve_problem(res, seed=6)
+    g = MGPCG(res, DEV, pre=3, post=3, stencil=stencil)
+    g.build_hierarchy(dev(bx), dev(by), dev(bz))
+    o = O.OracleMGPCG(res, pre=3, post=3, stencil=stencil)
+    o.build_hierarchy(bx, by, bz)
+    z = DeviceArray.zeros(res, device=DEV)
+    g.precondition(dev(b), z)
+    zo = o.precondition(b)
+    assert rel_err(z.numpy(), zo) < 2e-4
+    assert abs(float(z.numpy().astype(np.float64).mean())) < 1e-5 * np.abs(zo).max()
+
+
+@pytest.mark.parametrize("stencil,tol", [("flux", 1e-6), ("reference", 1e-5)])
+def test_solve_matches_oracle_iterations(stencil, tol):
+    """FP32 solve against the FP32 oracle of the same row form (iteration count
+    within one) and against the FP64 oracle (solution within 10*tol).  The
+    reference form stalls near 1.5e-6 here, so it is run to 1e-5."""
+    res = (32, 32, 32)
+    bx, by, bz, b, _ = scenes.solve_problem(res, seed=7)
+    g = MGPCG(res, DEV, pre=3, post=3, stencil=stencil)
+    g.build_hierarchy(dev(bx), dev(by), dev(bz))
+    x = DeviceArray.zeros(res, device=DEV)
+    it, rel = g.solve(dev(b), x, tol=tol, max_iter=100)
+    o = O.OracleMGPCG(res, pre=3, post=3, stencil=stencil)
+    o.build_hierarchy(bx, by, bz)
+    xo, ito, relo = o.solve(b, tol=tol, max_iter=100)
+    assert rel < tol and relo < tol, (rel, relo)
+    assert abs(it - ito) <= 1, (it, ito)
+    x64, _, _ = O.fp64_reference_solve(bx, by, bz, b.astype(np.float64), tol=1e-12)
+    assert rel_err(x.numpy(), x64) < 10 * tol
+    assert rel_err(xo, x64) < 10 * tol
+
+
+def test_flux_form_reaches_1e7_reference_form_stalls():
+    """The reason for the flux form: at 64^3 / 1000:1 the reference's row form
+    stalls above 1e-6 while the flux form reaches 1e-7 (same on the oracle)."""
+    res = (64, 64, 64)
+    bx, by, bz, b, _ = scenes.solve_problem(res, seed=8)
+    out = {}
+    for stencil in ("reference", "flux"):
+        g = MGPCG(res, DEV, pre=3, post=3, stencil=stencil)
+        g.build_hierarchy(dev(bx), dev(by), dev(bz))
+        x = DeviceArray.zeros(res, device=DEV)
+        out[stencil] = g.solve(dev(b), x, tol=1e-7, max_iter=60)
+    assert out["flux"][1] < 1e-7
+    assert out["reference"][1] > 1e-6
+
+
+def test_graph_and_eager_paths_are_bitwise_equal():
+    res = (32, 32, 32)
+    bx, by, bz, b, _ = scenes.solve_problem(res, seed=8)
+    outs = []
+    for graphs in (True, False, True):
+        g = MGPCG(res, DEV, pre=3, post=3, use_graphs=graphs)
+        g.build_hierarchy(dev(bx), dev(by), dev(bz))
+        x = DeviceArray.zeros(res, device=DEV)
+        outs.append((g.solve(dev(b), x, tol=1e-6, max_iter=100), x.numpy()))
+    assert outs[0][0] == outs[1][0] == outs[2][0]
+    assert np.array_equal(outs[0][1], outs[1][1]) and np.array_equal(outs[0][1], outs[2][1])
+
+
+def test_zero_rhs_and_max_iter():
+    res = (16, 16, 16)
+    bx, by, bz, b, _ = scenes.solve_problem(res, seed=9)
+    g = MGPCG(res, DEV)
+    g.build_hierarchy(dev(bx), dev(by), dev(bz))
+    x = dev(np.ones(res, np.float32))
+    assert g.solve(dev(np.zeros(res, np.float32)), x) == (0, 0.0)
+    assert np.abs(x.numpy()).max() == 0.0
+    it, rel = g.solve(dev(b), x, tol=1e-30, max_iter=3)
+    assert it == 3 and rel > 0.0
+    it0, rel0 = g.solve(dev(b), x, tol=1e-6, max_iter=0)
+    assert it0 == 0 and rel0 == 1.0
+
+
+def test_solver_reuse_across_sizes_and_repeated_calls():
+    res = (32, 32, 32)
+    bx, by, bz, b, _ = scenes.solve_problem(res, seed=10)
+    g = MGPCG(res, DEV, pre=3, post=3)
+    g.build_hierarchy(dev(bx), dev(by), dev(bz))
+    x1, x2 = DeviceArray.zeros(res, device=DEV), DeviceArray.zeros(res, device=DEV)
+    r1 = g.solve(dev(b), x1, tol=1e-6)
+    r2 = g.solve(dev(b), x2, tol=1e-6)
+    assert r1 == r2 and np.array_equal(x1.numpy(), x2.numpy())
