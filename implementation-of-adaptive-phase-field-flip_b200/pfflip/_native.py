@@ -81,7 +81,7 @@ SIGNATURES = {
     "pf_sort_workspace_bytes": (C.c_size_t, [_G, _I64]),
     "pf_sort_particles": (C.c_int, [_G, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, C.c_size_t, _VP]),
     "pf_p2g": (C.c_int, [_G, _I64, _VP, _VP, _VP, _F, _F, _F] + [_VP] * 8 + [_VP]),
-    "pf_phase_beta": (C.c_int, [_G] + [_VP] * 7 + [_VP] + [_F] * 6 + [_VP] * 15 + [_VP]),
+    "pf_phase_beta": (C.c_int, [_G] + [_VP] * 7 + [_VP] + [_F] * 6 + [_VP] * 14 + [_VP]),
     "pf_save_and_force": (C.c_int, [_G] + [_VP] * 6 + [_VP, _F, _F, _F, _F, _VP]),
     "pf_build_rhs": (C.c_int, [_G, _VP, _VP, _VP, _VP, _VP, _F, _F, _F, _VP]),
     "pf_project": (C.c_int, [_G, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _F, _VP]),

@@ -35,6 +35,26 @@ def test_python_binding_covers_header():
     assert not missing, missing
 
 
+def declared_arities():
+    out = {}
+    for fn in sorted(os.listdir(os.path.join(REPO, "include"))):
+        if not fn.endswith(".h"):
+            continue
+        src = open(os.path.join(REPO, "include", fn)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"\b(pf_[a-z0-9_]+)\s*\(([^)]*)\)\s*;", src):
+            args = m.group(2).strip()
+            out[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_binding_arities_match_header():
+    ar = declared_arities()
+    assert len(ar) >= 20
+    bad = {n: (a, len(N.SIGNATURES[n][1])) for n, a in ar.items() if len(N.SIGNATURES[n][1]) != a}
+    assert not bad, bad
+
+
 def test_host_only_entry_points():
     lib = N.lib()
     assert b"sm_100a" in lib.pf_version()
