@@ -1,0 +1,442 @@
+#!/usr/bin/env python3
+"""Benchmark of the uniform-grid PF-FLIP step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = one Simulator.step over the whole particle set): the
+128^3 dam break with 27 particles per cell (56,623,104 particles), liquid for
+x < 0.4 and y < 0.6, 1000:1 density, fixed dt = 0.5 dx / sqrt(2 g 0.6),
+MG-PCG to 1e-4 (the reference's production tolerance), plain FP32.  Seeding is
+the reference's jittered lattice from seed 42 (synthetic, no dataset).
+
+Printed (rank 0, one JSON line): steps/s of the whole job (``value``), the same
+metric end to end through the public API with the particle state uploaded from
+and read back to pinned host memory every step (``e2e``), the roofline of the
+dominant kernel from CUDA events in the timed region, SM clocks sampled during
+the timed region, this library's kernel launches in the timed region, the CPU
+oracle timed on a bounded sample (``cpu_baseline``), the standalone 128^3 MG-PCG
+solve to 1e-6 in FP32 and with the 16-bit hierarchy (``solve``), and the
+mixed-precision step (``mixed``).
+
+Multi-GPU: the step does not shard here (one GPU per simulation), so N ranks run
+N independent replicas (weak scaling, no data-path collective); the timing is
+the max over ranks.
+
+``--impl reference`` times the reference algorithm's CPU restatement (the
+oracle; NVIDIA Warp, the reference's runtime, is not installed) on the host
+cores with all threads, on the same workload and metric.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "implementation-of-adaptive-phase-field-flip_b200"))
+sys.path.insert(0, REPO)
+
+METRIC = "steps/s, dam_break 128^3 27ppc (56.6M particles) 1000:1, full PF-FLIP step"
+UNIT = "steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--res", type=int, default=128)
+    ap.add_argument("--ppc", type=int, default=27)
+    ap.add_argument("--tol", type=float, default=1e-4)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16", "bf16"])
+    ap.add_argument("--stencil", default="flux", choices=["flux", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--solve-oracle", action="store_true", help="also solve the 128^3 problem with the FP64 oracle")
+    return ap.parse_args()
+
+
+def workload_cfg(args, precision=None):
+    from pfflip import Config
+
+    r = args.res
+    return Config(res=(r, r, r), dx=1.0 / r, ppc=args.ppc, seed=42, droplets=False, pcg_tol=args.tol,
+                  precision=precision or args.precision, stencil=args.stencil)
+
+
+def fixed_dt(dx):
+    return 0.5 * dx / math.sqrt(2 * 9.81 * 0.6)
+
+
+def seed_particles(cfg):
+    from pfflip import scenes
+
+    return scenes.dam_break(cfg)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        exe = shutil.which("nvidia-smi")
+        if exe is None:
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.fh = open(self.path, "w")
+        self.proc = subprocess.Popen([exe, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                      "-i", str(self.gpu), "-lms", "100"], stdout=self.fh,
+                                     stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if self.proc is None:
+            return {"samples": 0, "note": "nvidia-smi unavailable"}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        for ln in open(self.path):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"samples": 0}
+        sm = np.array([r[0] for r in rows])
+        mx = max(r[1] for r in rows)
+        load = sm[sm > 0.5 * mx] if (sm > 0.5 * mx).any() else sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[3]) if v.lower().startswith("active")})
+        return {"sm_mhz": float(np.median(load)), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(r[2] for r in rows)}
+
+
+# ---------------------------------------------------------------- algorithmic bytes
+def algorithmic_bytes(stage, n_particles, n_cells, iters):
+    """Bytes each stage must move, counting every array once per launch (the
+    per-unit figures of the path's byte model; the float4 streams actually
+    move 32 B per particle and direction)."""
+    if stage == "p2g":  # read x,y,z,u,v,w + phase (25 B), write 8 accumulator grids (32 B/cell)
+        return 25 * n_particles + 32 * n_cells
+    if stage == "g2p_advect":  # read pos, vel, phase (25 B), write pos, vel (24 B); gathers L2-resident
+        return 49 * n_particles
+    if stage == "sort":  # key write+read x2, 25 B gather, 25 B scatter, 4 B permutation
+        return 70 * n_particles
+    if stage == "solve":  # ~ (V-cycle 205*8/7 + CG 68) B per cell and iteration
+        return (205 * 8 / 7 + 68) * n_cells * max(iters, 1)
+    return None
+
+
+def load_traffic():
+    p = os.path.join(REPO, "profiles", "traffic_per_unit.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p))
+        except Exception:
+            return {}
+    return {}
+
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- CPU oracle leg
+def cpu_oracle_steps(cfg, pos, vel, pt, nsteps, threads):
+    from oracle import oracle as O
+
+    O.set_threads(threads)
+    o = O.OracleSim(cfg, nthreads=threads, stencil=cfg.stencil)
+    o.set_particles(pos, vel, pt)
+    dt = fixed_dt(cfg.dx)
+    times = []
+    for _ in range(nsteps):
+        t0 = time.perf_counter()
+        o.step(dt)
+        times.append(time.perf_counter() - t0)
+    return times
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cfg = workload_cfg(args)
+    pos, vel, pt = seed_particles(cfg)
+    threads = os.cpu_count() or 1
+    steps = max(1, min(args.steps, 2))
+    warm = min(args.warmup, 1)
+    times = cpu_oracle_steps(cfg, pos, vel, pt, warm + steps, threads)[warm:]
+    v = len(times) / sum(times)
+    sample = (f"{len(times)} full oracle steps (after {warm} warm-up) of the {args.res}^3/{args.ppc}ppc dam break, "
+              f"{len(pos):,} particles; reference runtime NVIDIA Warp unavailable, so the CPU restatement of the "
+              f"reference kernels (oracle/pf_oracle.hpp) runs in its place")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": len(times), "warmup": warm, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic", "config": {"workload": f"dam_break {args.res}^3 {args.ppc}ppc"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU legs
+def run_ours(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    from pfflip import Simulator
+    from pfflip import _native as N
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    cfg = workload_cfg(args)
+    dt = fixed_dt(cfg.dx)
+    t_seed = time.perf_counter()
+    pos, vel, pt = seed_particles(cfg)
+    t_seed = time.perf_counter() - t_seed
+    n = len(pos)
+    ncell = cfg.res[0] * cfg.res[1] * cfg.res[2]
+
+    sim = Simulator(cfg)
+    sim.set_particles(pos, vel, pt)
+    for _ in range(args.warmup):
+        sim.step(dt)
+    sim.enable_stage_timing(True)
+    sim.stage_times(reset=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    l0 = N.launch_count()
+    e0.record(stream)
+    recs = [sim.step(dt) for _ in range(args.steps)]
+    e1.record(stream)
+    barrier()
+    launches = N.launch_count() - l0
+    clk = clocks.stop()
+    ms_local = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(ms_local)
+    stages = sim.stage_times(reset=True)
+    sim.enable_stage_timing(False)
+    iters = float(np.mean([r["pcg_iter"] for r in recs]))
+    value = world * 1000.0 / ms
+
+    # roofline of the dominant single-kernel stage
+    peak, peak_kind = peaks()
+    traffic_db = load_traffic()
+    per_stage = {k: {"launches": c, "ms_per_launch": t / c, "share": t / (ms_local * args.steps)}
+                 for k, (c, t) in stages.items()}
+    single = [k for k in ("p2g", "g2p_advect") if k in per_stage]
+    dom = max(single, key=lambda k: per_stage[k]["ms_per_launch"]) if single else None
+    roof = None
+    if dom:
+        ab = algorithmic_bytes(dom, n, ncell, iters)
+        dur = per_stage[dom]["ms_per_launch"] * 1e-3
+        ach = ab / dur / 1e9
+        tr = traffic_db.get(dom, {})
+        traffic = None
+        if "bytes_per_particle" in tr:
+            traffic = tr["bytes_per_particle"] * n + tr.get("bytes_per_cell", 0.0) * ncell
+        roof = {"kernel": {"p2g": "k_p2g", "g2p_advect": "k_g2p_advect"}[dom], "bound": "hbm", "achieved": ach,
+                "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": ab, "traffic": traffic}
+    for k, v in per_stage.items():
+        ab = algorithmic_bytes(k, n, ncell, iters)
+        if ab is not None:
+            v["achieved_gbs"] = ab / (v["ms_per_launch"] * 1e-3) / 1e9
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"dam_break {args.res}^3 {args.ppc}ppc", "res": args.res, "ppc": args.ppc,
+                   "particles": n, "dt": dt, "pcg_tol": args.tol, "precision": args.precision,
+                   "stencil": args.stencil, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (particle streams 2x1.8 GB)", "pcg_iter_mean": iters},
+        "clocks": clk, "gpu_launches": int(launches), "roofline": roof,
+        "stages_ms_per_step": {k: v["ms_per_launch"] * v["launches"] / args.steps for k, v in per_stage.items()},
+        "stages": per_stage, "seed_s": t_seed,
+    }
+
+    # end to end through the public API with host buffers
+    if not args.no_e2e:
+        hp = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+        hv = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+        ht = torch.from_numpy(pt.astype(np.int32)).pin_memory()
+        sim.read_particles(hp, hv)
+        torch.cuda.synchronize()
+        barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            sim.set_particles(hp, hv, ht)
+            sim.step(dt)
+            sim.read_particles(hp, hv)
+        f1.record(stream)
+        barrier()
+        ems = max_over_ranks(f0.elapsed_time(f1) / args.steps)
+        line["e2e"] = {"value": world * 1000.0 / ems, "unit": UNIT, "h2d_bytes_per_step": int(n * 28),
+                       "d2h_bytes_per_step": int(n * 24),
+                       "api": "Simulator.set_particles(pinned host) + step(dt) + read_particles(pinned host)"}
+
+    # standalone solve (128^3, tanh slab + sphere, 1000:1, N(0,1) rhs) to 1e-6
+    if not args.no_solve and rank == 0:
+        line["solve"] = solve_leg(args)
+
+    # mixed-precision step
+    if not args.no_mixed and rank == 0 and args.precision == "fp32":
+        del sim
+        torch.cuda.empty_cache()
+        line["mixed"] = mixed_leg(args, pos, vel, pt, dt, ms)
+
+    # CPU baseline: the oracle on a bounded sample of the same workload
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        times = cpu_oracle_steps(cfg, pos, vel, pt, 1, threads)
+        line["cpu_baseline"] = {"value": 1.0 / times[0], "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"1 full oracle step of the same {args.res}^3/{args.ppc}ppc dam break "
+                                          f"({n:,} particles), all host threads"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def solve_leg(args):
+    import torch
+
+    from pfflip import scenes
+    from pfflip._arrays import DeviceArray
+    from pfflip.poisson import MGPCG
+
+    r = args.res
+    bx, by, bz, b, _ = scenes.solve_problem((r, r, r), seed=42)
+    dev = lambda a: DeviceArray(torch.from_numpy(a).cuda())  # noqa: E731
+    out = {"workload": f"standalone solve {r}^3, 1000:1, tol 1e-6, pre=post=3"}
+    ref64 = None
+    if args.solve_oracle:
+        from oracle import oracle as O
+
+        ref64, _, _ = O.fp64_reference_solve(bx, by, bz, b.astype(np.float64), tol=1e-12)
+    for prec, stencil in (("fp32", "flux"), ("fp16", "flux"), ("bf16", "flux"), ("fp32", "reference")):
+        s = MGPCG((r, r, r), "cuda", pre=3, post=3, precision=prec, stencil=stencil)
+        s.build_hierarchy(dev(bx), dev(by), dev(bz))
+        x = DeviceArray.zeros((r, r, r))
+        bd = dev(b)
+        s.solve(bd, x, tol=1e-6, max_iter=100)  # warm-up (graph capture)
+        ts = []
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            it, rel = s.solve(bd, x, tol=1e-6, max_iter=100)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        rec = {"ms": float(np.median(ts)), "iters": it, "rel": rel, "converged": rel < 1e-6}
+        if ref64 is not None:
+            xv = x.numpy().astype(np.float64)
+            xv -= xv.mean()
+            rec["err_vs_fp64"] = float(np.abs(xv - ref64).max() / np.abs(ref64).max())
+        out[f"{prec}_{stencil}"] = rec
+        del s
+    return out
+
+
+def mixed_leg(args, pos, vel, pt, dt, ms_fp32):
+    import torch
+
+    from pfflip import Simulator
+
+    res = {}
+    for prec in ("fp16", "bf16"):
+        cfg = workload_cfg(args, precision=prec)
+        sim = Simulator(cfg)
+        sim.set_particles(pos, vel, pt)
+        for _ in range(args.warmup):
+            sim.step(dt)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        recs = [sim.step(dt) for _ in range(args.steps)]
+        e1.record()
+        torch.cuda.synchronize()
+        m = e0.elapsed_time(e1) / args.steps
+        res[prec] = {"ms_per_step": m, "steps_per_s": 1000.0 / m, "speedup_vs_fp32": ms_fp32 / m,
+                     "pcg_iter_mean": float(np.mean([r["pcg_iter"] for r in recs]))}
+        del sim
+        torch.cuda.empty_cache()
+    return res
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -56,7 +56,7 @@ static_assert(CNT_MAX <= PF_MG_COUNTERS, "counters");
 
 constexpr int RED_NT = 256;
 constexpr int RED_MAX_BLOCKS = 2 * kNumSMs * 4;  // 1184 partials per reduction
-constexpr int64_t kPartials = RED_MAX_BLOCKS * 2 * 4;
+constexpr int64_t kPartials = 1 << 16;  // >= CTAs of any one reduction (sweep tiles up to 512^3)
 
 __device__ __forceinline__ bool is_done(const MGState* st) { return st != nullptr && st->done != 0; }
 
@@ -176,13 +176,29 @@ __global__ void k_coarsen_faces(int fx, int fy, int fz, int cx, int cy, int cz, 
 }
 
 // --------------------------------------------------------------- fused red-black sweep
-constexpr int SW_TJ = 8, SW_TK = 32, SW_NT = SW_TJ * SW_TK;
-constexpr int SW_PJ = SW_TJ + 4, SW_PK = SW_TK + 4;  // p plane with 2-cell ring
-constexpr int SW_CJ = SW_TJ + 2, SW_CK = SW_TK + 2;  // coefficient plane with 1-cell ring
+// One CTA owns a TI x TJ x TK tile of cells.  It loads, with every load in
+// flight at once, p with a 2-cell halo and b and the three face arrays with a
+// 1-cell halo into shared memory (zero outside the level: boundary faces are
+// zero, so the stencil never sees the fill), updates colour 1 on the tile and
+// its 1-cell ring, then colour 2 on the tile, and writes the tile to p_out.
+// p_in and p_out are different buffers, so the halo a CTA reads is never
+// updated under it.  Within a row, thread q handles the q-th cell of the
+// colour being updated, so no lane idles on the other colour.
+constexpr int SW_TJ = 8, SW_TK = 32, SW_NT = 256;
+
+template <int TI> struct TileDims {
+  static constexpr int PI = TI + 4, PJ = SW_TJ + 4, PK = SW_TK + 4;  // p with 2-ring
+  static constexpr int CI = TI + 2, CJ = SW_TJ + 2, CK = SW_TK + 2;  // cells with 1-ring
+  static constexpr int PN = PI * PJ * PK;
+  static constexpr int CN = CI * CJ * CK;
+  static constexpr int XN = (CI + 1) * CJ * CK;
+  static constexpr int YN = CI * (CJ + 1) * CK;
+  static constexpr int ZN = CI * CJ * (CK + 1);
+  static constexpr size_t SMEM = sizeof(float) * (PN + CN + XN + YN + ZN);
+};
 
 template <class T, class TB> struct SweepArgs {
   int n0, n1, n2;
-  int ci;                  // planes per CTA along i
   const T* p_in;           // ignored when zero_in
   T* p_out;
   const TB* b;
@@ -203,144 +219,143 @@ template <class T, class TB> struct SweepArgs {
   int flux;                // PF_STENCIL_FLUX rows
 };
 
-__device__ __forceinline__ int mod3(int m) { return ((m % 3) + 3) % 3; }
+// Gauss-Seidel update of one cell from shared-memory neighbourhoods.
+// P: centre value pointer; sP[...] strides; faces and b passed in.
+__device__ __forceinline__ float gs_update(float pv, float pxl, float pxu, float pyl, float pyu, float pzl, float pzu,
+                                           float bxl, float bxu, float byl, float byu, float bzl, float bzu, float bb,
+                                           float omega, int flux, bool* ok) {
+  const float d = bxl + bxu + byl + byu + bzl + bzu;
+  *ok = d > 0.f;
+  float res;
+  if (flux) {
+    float sum = bxl * (pv - pxl);
+    sum += bxu * (pv - pxu);
+    sum += byl * (pv - pyl);
+    sum += byu * (pv - pyu);
+    sum += bzl * (pv - pzl);
+    sum += bzu * (pv - pzu);
+    res = bb - sum;
+  } else {
+    float sum = bxl * pxl;
+    sum += bxu * pxu;
+    sum += byl * pyl;
+    sum += byu * pyu;
+    sum += bzl * pzl;
+    sum += bzu * pzu;
+    res = bb - (d * pv - sum);
+  }
+  return pv + omega * res / d;
+}
 
-template <class T, class TB>
-__global__ void __launch_bounds__(SW_NT) k_rb_sweep(SweepArgs<T, TB> a) {
+template <class T, class TB, int TI>
+__global__ void __launch_bounds__(SW_NT) k_rb_tile(SweepArgs<T, TB> a) {
   if (is_done(a.st)) return;
-  __shared__ float sP[4][SW_PJ][SW_PK];
-  __shared__ float sB[2][SW_CJ][SW_CK];
-  __shared__ float sBY[2][SW_CJ + 1][SW_CK];
-  __shared__ float sBZ[2][SW_CJ][SW_CK + 1];
-  __shared__ float sBX[3][SW_CJ][SW_CK];
+  using D = TileDims<TI>;
+  extern __shared__ __align__(16) float smem[];
+  float* sP = smem;
+  float* sB = sP + D::PN;
+  float* sX = sB + D::CN;
+  float* sY = sX + D::XN;
+  float* sZ = sY + D::YN;
   __shared__ double sred[40];
 
   const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
-  const int k0 = blockIdx.x * SW_TK, j0 = blockIdx.y * SW_TJ;
-  const int ia = blockIdx.z * a.ci, ib = min(n0, ia + a.ci);
+  const int k0 = blockIdx.x * SW_TK, j0 = blockIdx.y * SW_TJ, i0 = blockIdx.z * TI;
   const int tid = threadIdx.x;
   const long long sI = (long long)n1 * n2;
   const float bsc = a.b_scale ? *a.b_scale : 1.f;
-  const int c1 = a.first_color, c2 = a.first_color ^ 1;
   const int hn1 = n1 >> 1, hn2 = n2 >> 1;
 
-  auto load_p_plane = [&](int i) {
-    float(*P)[SW_PK] = sP[i & 3];
-    for (int e = tid; e < SW_PJ * SW_PK; e += SW_NT) {
-      const int r = e / SW_PK, c = e % SW_PK;
-      const int j = j0 - 2 + r, k = k0 - 2 + c;
-      float v = 0.f;
-      if (i >= 0 && i < n0 && j >= 0 && j < n1 && k >= 0 && k < n2) {
-        const long long g = i * sI + (long long)j * n2 + k;
-        if (!a.zero_in) v = ldT(a.p_in + g);
-        if (a.pc) v += ldT(a.pc + ((long long)(i >> 1) * hn1 + (j >> 1)) * hn2 + (k >> 1)) * a.pc_scale;
-      }
-      P[r][c] = v;
+  // ---- loads (zero outside the level)
+  for (int e = tid; e < D::PN; e += SW_NT) {
+    const int c = e % D::PK, t = e / D::PK, r = t % D::PJ, q = t / D::PJ;
+    const int i = i0 - 2 + q, j = j0 - 2 + r, k = k0 - 2 + c;
+    float v = 0.f;
+    if (i >= 0 && i < n0 && j >= 0 && j < n1 && k >= 0 && k < n2) {
+      const long long g = i * sI + (long long)j * n2 + k;
+      if (!a.zero_in) v = ldT(a.p_in + g);
+      if (a.pc) v += ldT(a.pc + ((long long)(i >> 1) * hn1 + (j >> 1)) * hn2 + (k >> 1)) * a.pc_scale;
     }
-  };
-  auto load_cell_coefs = [&](int i) {  // b, by, bz of cell plane i
-    const int s = i & 1;
-    const bool iin = (i >= 0 && i < n0);
-    for (int e = tid; e < SW_CJ * SW_CK; e += SW_NT) {
-      const int r = e / SW_CK, c = e % SW_CK;
-      const int j = j0 - 1 + r, k = k0 - 1 + c;
-      const bool in = iin && j >= 0 && j < n1 && k >= 0 && k < n2;
-      sB[s][r][c] = in ? ldT(a.b + i * sI + (long long)j * n2 + k) * bsc : 0.f;
-    }
-    for (int e = tid; e < (SW_CJ + 1) * SW_CK; e += SW_NT) {
-      const int r = e / SW_CK, c = e % SW_CK;
-      const int j = j0 - 1 + r, k = k0 - 1 + c;
-      const bool in = iin && j >= 0 && j <= n1 && k >= 0 && k < n2;
-      sBY[s][r][c] = in ? ldT(a.by + ((long long)i * (n1 + 1) + j) * n2 + k) : 0.f;
-    }
-    for (int e = tid; e < SW_CJ * (SW_CK + 1); e += SW_NT) {
-      const int r = e / (SW_CK + 1), c = e % (SW_CK + 1);
-      const int j = j0 - 1 + r, k = k0 - 1 + c;
-      const bool in = iin && j >= 0 && j < n1 && k >= 0 && k <= n2;
-      sBZ[s][r][c] = in ? ldT(a.bz + ((long long)i * n1 + j) * (n2 + 1) + k) : 0.f;
-    }
-  };
-  auto load_bx_plane = [&](int f) {  // x-faces of plane f (between cells f-1 and f)
-    float(*X)[SW_CK] = sBX[mod3(f)];
-    const bool fin = (f >= 0 && f <= n0);
-    for (int e = tid; e < SW_CJ * SW_CK; e += SW_NT) {
-      const int r = e / SW_CK, c = e % SW_CK;
-      const int j = j0 - 1 + r, k = k0 - 1 + c;
-      const bool in = fin && j >= 0 && j < n1 && k >= 0 && k < n2;
-      X[r][c] = in ? ldT(a.bx + (long long)f * sI + (long long)j * n2 + k) : 0.f;
-    }
-  };
-  // one Gauss-Seidel update of cell (m, r-1, c-1) of the coefficient frame
-  auto relax = [&](int m, int r, int c) {
-    float(*Pm)[SW_PK] = sP[m & 3];
-    const float(*Pl)[SW_PK] = sP[(m - 1) & 3];
-    const float(*Pu)[SW_PK] = sP[(m + 1) & 3];
-    const int s = m & 1;
-    const float bxl = sBX[mod3(m)][r][c], bxu = sBX[mod3(m + 1)][r][c];
-    const float byl = sBY[s][r][c], byu = sBY[s][r + 1][c];
-    const float bzl = sBZ[s][r][c], bzu = sBZ[s][r][c + 1];
-    const float d = bxl + bxu + byl + byu + bzl + bzu;
-    if (!(d > 0.f)) return;
-    const int pr = r + 1, pc = c + 1;
-    const float pv = Pm[pr][pc];
-    float res;
-    if (a.flux) {
-      float sum = bxl * (pv - Pl[pr][pc]);
-      sum += bxu * (pv - Pu[pr][pc]);
-      sum += byl * (pv - Pm[pr - 1][pc]);
-      sum += byu * (pv - Pm[pr + 1][pc]);
-      sum += bzl * (pv - Pm[pr][pc - 1]);
-      sum += bzu * (pv - Pm[pr][pc + 1]);
-      res = sB[s][r][c] - sum;
-    } else {
-      float sum = bxl * Pl[pr][pc];
-      sum += bxu * Pu[pr][pc];
-      sum += byl * Pm[pr - 1][pc];
-      sum += byu * Pm[pr + 1][pc];
-      sum += bzl * Pm[pr][pc - 1];
-      sum += bzu * Pm[pr][pc + 1];
-      res = sB[s][r][c] - (d * pv - sum);
-    }
-    Pm[pr][pc] = pv + a.omega * res / d;
-  };
-
-  // prologue: p planes ia-2, ia-1 and x-face plane ia-1
-  load_p_plane(ia - 2);
-  load_p_plane(ia - 1);
-  load_bx_plane(ia - 1);
-  double msum = 0.0;
-  const int ty = tid / SW_TK, tx = tid % SW_TK;
-
-  for (int m = ia - 1; m <= ib; ++m) {
-    load_p_plane(m + 1);
-    load_cell_coefs(m);
-    load_bx_plane(m + 1);
-    __syncthreads();
-    // colour 1 on plane m over the tile and its 1-cell ring
-    if (m >= 0 && m < n0) {
-      for (int e = tid; e < SW_CJ * SW_CK; e += SW_NT) {
-        const int r = e / SW_CK, c = e % SW_CK;
-        const int j = j0 - 1 + r, k = k0 - 1 + c;
-        if (j < 0 || j >= n1 || k < 0 || k >= n2) continue;
-        if (((m + j + k) & 1) != c1) continue;
-        relax(m, r, c);
-      }
-    }
-    __syncthreads();
-    // colour 2 on plane m-1 over the tile, then write the plane
-    const int mb = m - 1;
-    if (mb >= ia && mb < ib) {
-      const int j = j0 + ty, k = k0 + tx;
-      if (j < n1 && k < n2) {
-        if (((mb + j + k) & 1) == c2) relax(mb, ty + 1, tx + 1);
-        const float v = sP[mb & 3][ty + 2][tx + 2];
-        stT(a.p_out + mb * sI + (long long)j * n2 + k, v);
-        if (a.partials) msum += (double)roundT<T>(v);
-      }
-    }
-    __syncthreads();
+    sP[e] = v;
   }
+  for (int e = tid; e < D::CN; e += SW_NT) {
+    const int c = e % D::CK, t = e / D::CK, r = t % D::CJ, q = t / D::CJ;
+    const int i = i0 - 1 + q, j = j0 - 1 + r, k = k0 - 1 + c;
+    const bool in = i >= 0 && i < n0 && j >= 0 && j < n1 && k >= 0 && k < n2;
+    sB[e] = in ? ldT(a.b + i * sI + (long long)j * n2 + k) * bsc : 0.f;
+  }
+  for (int e = tid; e < D::XN; e += SW_NT) {  // x-faces i0-1 .. i0+TI+1
+    const int c = e % D::CK, t = e / D::CK, r = t % D::CJ, q = t / D::CJ;
+    const int f = i0 - 1 + q, j = j0 - 1 + r, k = k0 - 1 + c;
+    const bool in = f >= 0 && f <= n0 && j >= 0 && j < n1 && k >= 0 && k < n2;
+    sX[e] = in ? ldT(a.bx + (long long)f * sI + (long long)j * n2 + k) : 0.f;
+  }
+  for (int e = tid; e < D::YN; e += SW_NT) {  // y-faces j0-1 .. j0+TJ+1
+    const int c = e % D::CK, t = e / D::CK, r = t % (D::CJ + 1), q = t / (D::CJ + 1);
+    const int i = i0 - 1 + q, f = j0 - 1 + r, k = k0 - 1 + c;
+    const bool in = i >= 0 && i < n0 && f >= 0 && f <= n1 && k >= 0 && k < n2;
+    sY[e] = in ? ldT(a.by + ((long long)i * (n1 + 1) + f) * n2 + k) : 0.f;
+  }
+  for (int e = tid; e < D::ZN; e += SW_NT) {  // z-faces k0-1 .. k0+TK+1
+    const int c = e % (D::CK + 1), t = e / (D::CK + 1), r = t % D::CJ, q = t / D::CJ;
+    const int i = i0 - 1 + q, j = j0 - 1 + r, f = k0 - 1 + c;
+    const bool in = i >= 0 && i < n0 && j >= 0 && j < n1 && f >= 0 && f <= n2;
+    sZ[e] = in ? ldT(a.bz + ((long long)i * n1 + j) * (n2 + 1) + f) : 0.f;
+  }
+  __syncthreads();
 
+  // relax the cell at coefficient-frame coordinates (q, r, c)
+  auto relax = [&](int q, int r, int c) {
+    float* pp = sP + ((q + 1) * D::PJ + (r + 1)) * D::PK + (c + 1);
+    const int ce = (q * D::CJ + r) * D::CK + c;
+    const float bxl = sX[ce], bxu = sX[ce + D::CJ * D::CK];
+    const int ye = (q * (D::CJ + 1) + r) * D::CK + c;
+    const float byl = sY[ye], byu = sY[ye + D::CK];
+    const int ze = (q * D::CJ + r) * (D::CK + 1) + c;
+    const float bzl = sZ[ze], bzu = sZ[ze + 1];
+    bool ok;
+    const float v = gs_update(*pp, pp[-D::PJ * D::PK], pp[D::PJ * D::PK], pp[-D::PK], pp[D::PK], pp[-1], pp[1], bxl,
+                              bxu, byl, byu, bzl, bzu, sB[ce], a.omega, a.flux, &ok);
+    if (ok) *pp = v;
+  };
+
+  // ---- colour 1 on the tile and its ring: per row of CK cells, CK/2 cells of the colour
+  const int c1 = a.first_color, c2 = c1 ^ 1;
+  {
+    constexpr int HALF = D::CK / 2;  // 17
+    for (int e = tid; e < D::CI * D::CJ * HALF; e += SW_NT) {
+      const int h = e % HALF, row = e / HALF, r = row % D::CJ, q = row / D::CJ;
+      const int i = i0 - 1 + q, j = j0 - 1 + r;
+      const int par = (c1 - i - j - (k0 - 1)) & 1;
+      const int c = 2 * h + par, k = k0 - 1 + c;
+      if (i < 0 || i >= n0 || j < 0 || j >= n1 || k < 0 || k >= n2) continue;
+      relax(q, r, c);
+    }
+  }
+  __syncthreads();
+  // ---- colour 2 on the tile
+  {
+    constexpr int HALF = SW_TK / 2;  // 16
+    for (int e = tid; e < TI * SW_TJ * HALF; e += SW_NT) {
+      const int h = e % HALF, row = e / HALF, r = row % SW_TJ, q = row / SW_TJ;
+      const int i = i0 + q, j = j0 + r;
+      const int par = (c2 - i - j - k0) & 1;
+      const int c = 2 * h + par, k = k0 + c;
+      if (i >= n0 || j >= n1 || k >= n2) continue;
+      relax(q + 1, r + 1, c + 1);
+    }
+  }
+  __syncthreads();
+  // ---- write the tile
+  double msum = 0.0;
+  for (int e = tid; e < TI * SW_TJ * SW_TK; e += SW_NT) {
+    const int c = e % SW_TK, t = e / SW_TK, r = t % SW_TJ, q = t / SW_TJ;
+    const int i = i0 + q, j = j0 + r, k = k0 + c;
+    if (i >= n0 || j >= n1 || k >= n2) continue;
+    const float v = sP[((q + 2) * D::PJ + (r + 2)) * D::PK + (c + 2)];
+    stT(a.p_out + i * sI + (long long)j * n2 + k, v);
+    if (a.partials) msum += (double)roundT<T>(v);
+  }
   if (a.partials) {
     const double bs = block_sum<SW_NT>(msum, sred);
     const int nb = gridDim.x * gridDim.y * gridDim.z;
@@ -426,14 +441,251 @@ __global__ void k_residual_restrict(int n0, int n1, int n2, const T* __restrict_
   }
 }
 
-// --------------------------------------------------------------- coarsest level
-// The coarsest level runs `coarsest` red-black sweeps from p = 0 followed by
-// mean removal (pfflip/poisson.py:325-328) in one CTA with the level in shared
-// memory (levels up to kCoarseMaxCells cells; larger ones use the sweep
-// kernel).  Arithmetic in AccT: float reproduces the reference, double is the
-// FP64 coarsest solve of the 16-bit hierarchy.  Kernel: k_coarsest_b below.
-constexpr int kCoarseMaxCells = 4096;
-constexpr int CO_NT = 512;
+// --------------------------------------------------------------- bottom of the V-cycle
+// All levels from `lb` down (each <= kBottomMaxCells cells) run inside one CTA
+// with the levels in shared memory: pre-smoothing, residual + restriction,
+// the coarsest solve (`coarsest` sweeps from zero, then mean removal,
+// pfflip/poisson.py:325-328), prolongation and post-smoothing, exactly the
+// reference's recursion (pfflip/poisson.py:323-343) with in-place red/black
+// half-sweeps separated by barriers.  Replaces ~7 launches per level.  The
+// coarsest level runs in AccT (float reproduces the reference; double is the
+// FP64 coarsest solve of the 16-bit hierarchy), by one warp when it has at most
+// 256 cells.
+constexpr int kBottomMaxCells = 4096;
+constexpr int BT_NT = 1024;
+
+struct BottomLevel {
+  int n0, n1, n2;
+  const void* bx;
+  const void* by;
+  const void* bz;
+};
+
+template <class T, class TB> struct BottomArgs {
+  int nl;                           // bottom levels, [0] = top
+  BottomLevel L[PF_MG_MAX_LEVELS];
+  const TB* b;                      // right-hand side of the top bottom level
+  const float* b_scale;
+  T* p_out;                         // solution of the top bottom level
+  float omega;
+  int pre, post, coarsest;
+  float rscale, pscale;
+  int flux;
+  MGState* st;
+  int want_mean, mixed;
+};
+
+__host__ __device__ inline size_t bottom_level_floats(int n0, int n1, int n2) {
+  const size_t n = (size_t)n0 * n1 * n2;
+  return 2 * n + (size_t)(n0 + 1) * n1 * n2 + (size_t)n0 * (n1 + 1) * n2 + (size_t)n0 * n1 * (n2 + 1);
+}
+
+// in-place relax of cell (i,j,k) of a shared-memory level, clamped neighbours
+template <class R>
+__device__ __forceinline__ void bt_relax(R* P, const float* B, const float* X, const float* Y, const float* Z, int n0,
+                                         int n1, int n2, int i, int j, int k, R omega, int flux) {
+  const int sI = n1 * n2, e = (i * n1 + j) * n2 + k;
+  const int fyi = (i * (n1 + 1) + j) * n2 + k, fzi = (i * n1 + j) * (n2 + 1) + k;
+  const R bxl = X[e], bxu = X[e + sI], byl = Y[fyi], byu = Y[fyi + n2], bzl = Z[fzi], bzu = Z[fzi + 1];
+  const R d = (R)(X[e] + X[e + sI] + Y[fyi] + Y[fyi + n2] + Z[fzi] + Z[fzi + 1]);
+  if (!(d > R(0))) return;
+  const R pv = P[e];
+  const R q0 = P[i > 0 ? e - sI : e], q1 = P[i < n0 - 1 ? e + sI : e];
+  const R q2 = P[j > 0 ? e - n2 : e], q3 = P[j < n1 - 1 ? e + n2 : e];
+  const R q4 = P[k > 0 ? e - 1 : e], q5 = P[k < n2 - 1 ? e + 1 : e];
+  R res;
+  if (flux) {
+    R sum = bxl * (pv - q0);
+    sum += bxu * (pv - q1);
+    sum += byl * (pv - q2);
+    sum += byu * (pv - q3);
+    sum += bzl * (pv - q4);
+    sum += bzu * (pv - q5);
+    res = (R)B[e] - sum;
+  } else {
+    R sum = bxl * q0;
+    sum += bxu * q1;
+    sum += byl * q2;
+    sum += byu * q3;
+    sum += bzl * q4;
+    sum += bzu * q5;
+    res = (R)B[e] - (d * pv - sum);
+  }
+  P[e] = pv + omega * res / d;
+}
+
+template <class T, class TB, class AccT>
+__global__ void __launch_bounds__(BT_NT) k_bottom(BottomArgs<T, TB> a) {
+  if (is_done(a.st)) return;
+  extern __shared__ __align__(16) unsigned char btsm[];
+  __shared__ double sred[40];
+  __shared__ double s_mean;
+  const int tid = threadIdx.x;
+  // carve the levels
+  float* Pl[PF_MG_MAX_LEVELS];
+  float* Bl[PF_MG_MAX_LEVELS];
+  float* Xl[PF_MG_MAX_LEVELS];
+  float* Yl[PF_MG_MAX_LEVELS];
+  float* Zl[PF_MG_MAX_LEVELS];
+  {
+    float* cur = reinterpret_cast<float*>(btsm);
+    for (int l = 0; l < a.nl; ++l) {
+      const int n0 = a.L[l].n0, n1 = a.L[l].n1, n2 = a.L[l].n2, n = n0 * n1 * n2;
+      Pl[l] = cur; cur += n;
+      Bl[l] = cur; cur += n;
+      Xl[l] = cur; cur += (n0 + 1) * n1 * n2;
+      Yl[l] = cur; cur += n0 * (n1 + 1) * n2;
+      Zl[l] = cur; cur += n0 * n1 * (n2 + 1);
+    }
+  }
+  AccT* Pc;  // coarsest level in AccT, after the float levels
+  {
+    const BottomLevel& Lc = a.L[a.nl - 1];
+    float* end = Zl[a.nl - 1] + Lc.n0 * Lc.n1 * (Lc.n2 + 1);
+    uintptr_t u = (reinterpret_cast<uintptr_t>(end) + 15) & ~uintptr_t(15);
+    Pc = reinterpret_cast<AccT*>(u);
+  }
+  // load faces of every level and b of the top level; zero p
+  const float bsc = a.b_scale ? *a.b_scale : 1.f;
+  for (int l = 0; l < a.nl; ++l) {
+    const int n0 = a.L[l].n0, n1 = a.L[l].n1, n2 = a.L[l].n2, n = n0 * n1 * n2;
+    const int nfx = (n0 + 1) * n1 * n2, nfy = n0 * (n1 + 1) * n2, nfz = n0 * n1 * (n2 + 1);
+    const T* gx = reinterpret_cast<const T*>(a.L[l].bx);
+    const T* gy = reinterpret_cast<const T*>(a.L[l].by);
+    const T* gz = reinterpret_cast<const T*>(a.L[l].bz);
+    for (int e = tid; e < nfx; e += BT_NT) Xl[l][e] = ldT(gx + e);
+    for (int e = tid; e < nfy; e += BT_NT) Yl[l][e] = ldT(gy + e);
+    for (int e = tid; e < nfz; e += BT_NT) Zl[l][e] = ldT(gz + e);
+    for (int e = tid; e < n; e += BT_NT) Pl[l][e] = 0.f;
+  }
+  {
+    const int n = a.L[0].n0 * a.L[0].n1 * a.L[0].n2;
+    for (int e = tid; e < n; e += BT_NT) Bl[0][e] = ldT(a.b + e) * bsc;
+  }
+  __syncthreads();
+  const float om = a.omega;
+  auto smooth = [&](int l, int nsweeps, int first) {
+    const int n0 = a.L[l].n0, n1 = a.L[l].n1, n2 = a.L[l].n2, n = n0 * n1 * n2;
+    for (int s = 0; s < nsweeps; ++s) {
+      for (int cc = 0; cc < 2; ++cc) {
+        const int color = first ^ cc;
+        for (int e = tid; e < n; e += BT_NT) {
+          const int k = e % n2, t = e / n2, j = t % n1, i = t / n1;
+          if (((i + j + k) & 1) != color) continue;
+          bt_relax<float>(Pl[l], Bl[l], Xl[l], Yl[l], Zl[l], n0, n1, n2, i, j, k, om, a.flux);
+        }
+        __syncthreads();
+      }
+    }
+  };
+  // ---- down
+  for (int l = 0; l < a.nl - 1; ++l) {
+    smooth(l, a.pre, 0);
+    const int n0 = a.L[l].n0, n1 = a.L[l].n1, n2 = a.L[l].n2;
+    const int C0 = n0 >> 1, C1 = n1 >> 1, C2 = n2 >> 1, nc = C0 * C1 * C2;
+    const float* P = Pl[l];
+    const float* B = Bl[l];
+    const float* X = Xl[l];
+    const float* Y = Yl[l];
+    const float* Z = Zl[l];
+    const int sI = n1 * n2;
+    for (int ec = tid; ec < nc; ec += BT_NT) {
+      const int K = ec % C2, t = ec / C2, J = t % C1, I = t / C1;
+      float acc = 0.f;
+      for (int aa = 0; aa < 2; ++aa)
+        for (int bb = 0; bb < 2; ++bb)
+          for (int cc = 0; cc < 2; ++cc) {
+            const int i = 2 * I + aa, j = 2 * J + bb, k = 2 * K + cc;
+            const int e = (i * n1 + j) * n2 + k;
+            const int fyi = (i * (n1 + 1) + j) * n2 + k, fzi = (i * n1 + j) * (n2 + 1) + k;
+            const float bxl = X[e], bxu = X[e + sI], byl = Y[fyi], byu = Y[fyi + n2], bzl = Z[fzi], bzu = Z[fzi + 1];
+            const float pv = P[e];
+            const float q0 = P[i > 0 ? e - sI : e], q1 = P[i < n0 - 1 ? e + sI : e];
+            const float q2 = P[j > 0 ? e - n2 : e], q3 = P[j < n1 - 1 ? e + n2 : e];
+            const float q4 = P[k > 0 ? e - 1 : e], q5 = P[k < n2 - 1 ? e + 1 : e];
+            float Ap;
+            if (a.flux) {
+              float sm = bxl * (pv - q0);
+              sm += bxu * (pv - q1);
+              sm += byl * (pv - q2);
+              sm += byu * (pv - q3);
+              sm += bzl * (pv - q4);
+              sm += bzu * (pv - q5);
+              Ap = sm;
+            } else {
+              const float d = bxl + bxu + byl + byu + bzl + bzu;
+              float sm = bxl * q0;
+              sm += bxu * q1;
+              sm += byl * q2;
+              sm += byu * q3;
+              sm += bzl * q4;
+              sm += bzu * q5;
+              Ap = d * pv - sm;
+            }
+            acc += B[e] - Ap;
+          }
+      Bl[l + 1][ec] = roundT<T>(acc * a.rscale);
+    }
+    __syncthreads();
+  }
+  // ---- coarsest
+  {
+    const int l = a.nl - 1;
+    const int n0 = a.L[l].n0, n1 = a.L[l].n1, n2 = a.L[l].n2, n = n0 * n1 * n2;
+    for (int e = tid; e < n; e += BT_NT) Pc[e] = AccT(0);
+    __syncthreads();
+    const bool one_warp = n <= 256;
+    const AccT omc = (AccT)om;
+    if (!one_warp || tid < 32) {
+      const int nt = one_warp ? 32 : BT_NT;
+      for (int s = 0; s < a.coarsest; ++s) {
+        for (int color = 0; color < 2; ++color) {
+          for (int e = tid; e < n; e += nt) {
+            const int k = e % n2, t = e / n2, j = t % n1, i = t / n1;
+            if (((i + j + k) & 1) != color) continue;
+            bt_relax<AccT>(Pc, Bl[l], Xl[l], Yl[l], Zl[l], n0, n1, n2, i, j, k, omc, a.flux);
+          }
+          if (one_warp) __syncwarp();
+          else __syncthreads();
+        }
+      }
+    }
+    __syncthreads();
+    double ls = 0.0;
+    for (int e = tid; e < n; e += BT_NT) ls += (double)Pc[e];
+    const double tot = block_sum<BT_NT>(ls, sred);
+    if (tid == 0) s_mean = tot / (double)n;
+    __syncthreads();
+    const AccT shift = (AccT)(-s_mean);
+    for (int e = tid; e < n; e += BT_NT) Pl[l][e] = roundT<T>((float)(Pc[e] + shift));
+    __syncthreads();
+  }
+  // ---- up
+  for (int l = a.nl - 2; l >= 0; --l) {
+    const int n0 = a.L[l].n0, n1 = a.L[l].n1, n2 = a.L[l].n2, n = n0 * n1 * n2;
+    const int h1 = n1 >> 1, h2 = n2 >> 1;
+    for (int e = tid; e < n; e += BT_NT) {
+      const int k = e % n2, t = e / n2, j = t % n1, i = t / n1;
+      Pl[l][e] += Pl[l + 1][((i >> 1) * h1 + (j >> 1)) * h2 + (k >> 1)] * a.pscale;
+    }
+    __syncthreads();
+    smooth(l, a.post, 1);
+  }
+  // ---- output (and the mean when the top level is level 0)
+  const int n = a.L[0].n0 * a.L[0].n1 * a.L[0].n2;
+  double ls = 0.0;
+  for (int e = tid; e < n; e += BT_NT) {
+    stT(a.p_out + e, Pl[0][e]);
+    ls += (double)roundT<T>(Pl[0][e]);
+  }
+  if (a.want_mean) {
+    const double tot = block_sum<BT_NT>(ls, sred);
+    if (tid == 0) {
+      a.st->sum_last = tot;
+      a.st->c_shift = (float)(-(tot / (double)n) * (a.mixed ? (double)a.st->zscale : 1.0));
+    }
+  }
+}
 
 // --------------------------------------------------------------- CG vector kernels
 // Sum of b (for the mean); last CTA stores c_shift = float(-sum/n).
@@ -718,84 +970,6 @@ __global__ void k_clear_done(MGState* st) {
   st->status = ST_RUNNING;
 }
 
-// coarsest level in one CTA, b possibly of another storage type (level 0)
-template <class T, class TB, class AccT>
-__global__ void __launch_bounds__(CO_NT) k_coarsest_b(int n0, int n1, int n2, const TB* __restrict__ b,
-                                                      const float* b_scale, const T* __restrict__ bx,
-                                                      const T* __restrict__ by, const T* __restrict__ bz,
-                                                      T* __restrict__ p_out, int sweeps, float omega, MGState* st,
-                                                      int flux) {
-  if (is_done(st)) return;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  const int n = n0 * n1 * n2;
-  const int nfx = (n0 + 1) * n1 * n2, nfy = n0 * (n1 + 1) * n2, nfz = n0 * n1 * (n2 + 1);
-  AccT* P = reinterpret_cast<AccT*>(smraw);
-  AccT* B = P + n;
-  AccT* D = B + n;
-  float* X = reinterpret_cast<float*>(D + n);
-  float* Y = X + nfx;
-  float* Z = Y + nfy;
-  __shared__ double sred[40];
-  const int tid = threadIdx.x;
-  const float bsc = b_scale ? *b_scale : 1.f;
-  for (int e = tid; e < n; e += CO_NT) { P[e] = AccT(0); B[e] = (AccT)(ldT(b + e) * bsc); }
-  for (int e = tid; e < nfx; e += CO_NT) X[e] = ldT(bx + e);
-  for (int e = tid; e < nfy; e += CO_NT) Y[e] = ldT(by + e);
-  for (int e = tid; e < nfz; e += CO_NT) Z[e] = ldT(bz + e);
-  __syncthreads();
-  const int sI = n1 * n2;
-  for (int e = tid; e < n; e += CO_NT) {
-    const int k = e % n2, t = e / n2, j = t % n1, i = t / n1;
-    const int fyi = (i * (n1 + 1) + j) * n2 + k, fzi = (i * n1 + j) * (n2 + 1) + k;
-    D[e] = (AccT)(X[e] + X[e + sI] + Y[fyi] + Y[fyi + n2] + Z[fzi] + Z[fzi + 1]);
-  }
-  __syncthreads();
-  const AccT om = (AccT)omega;
-  for (int s = 0; s < sweeps; ++s) {
-    for (int color = 0; color < 2; ++color) {
-      for (int e = tid; e < n; e += CO_NT) {
-        const int k = e % n2, t = e / n2, j = t % n1, i = t / n1;
-        if (((i + j + k) & 1) != color) continue;
-        const AccT d = D[e];
-        if (!(d > AccT(0))) continue;
-        const int fyi = (i * (n1 + 1) + j) * n2 + k, fzi = (i * n1 + j) * (n2 + 1) + k;
-        const AccT pv = P[e];
-        const AccT q0 = P[i > 0 ? e - sI : e], q1 = P[i < n0 - 1 ? e + sI : e];
-        const AccT q2 = P[j > 0 ? e - n2 : e], q3 = P[j < n1 - 1 ? e + n2 : e];
-        const AccT q4 = P[k > 0 ? e - 1 : e], q5 = P[k < n2 - 1 ? e + 1 : e];
-        AccT res;
-        if (flux) {
-          AccT sum = (AccT)X[e] * (pv - q0);
-          sum += (AccT)X[e + sI] * (pv - q1);
-          sum += (AccT)Y[fyi] * (pv - q2);
-          sum += (AccT)Y[fyi + n2] * (pv - q3);
-          sum += (AccT)Z[fzi] * (pv - q4);
-          sum += (AccT)Z[fzi + 1] * (pv - q5);
-          res = B[e] - sum;
-        } else {
-          AccT sum = (AccT)X[e] * q0;
-          sum += (AccT)X[e + sI] * q1;
-          sum += (AccT)Y[fyi] * q2;
-          sum += (AccT)Y[fyi + n2] * q3;
-          sum += (AccT)Z[fzi] * q4;
-          sum += (AccT)Z[fzi + 1] * q5;
-          res = B[e] - (d * pv - sum);
-        }
-        P[e] += om * res / d;
-      }
-      __syncthreads();
-    }
-  }
-  double ls = 0.0;
-  for (int e = tid; e < n; e += CO_NT) ls += (double)P[e];
-  const double tot = block_sum<CO_NT>(ls, sred);
-  __shared__ double s_mean;
-  if (tid == 0) s_mean = tot / (double)n;
-  __syncthreads();
-  const AccT shift = (AccT)(-s_mean);
-  for (int e = tid; e < n; e += CO_NT) stT(p_out + e, (float)(P[e] + shift));
-}
-
 // =============================================================== host side
 void count_suppress(bool on);
 
@@ -805,7 +979,8 @@ struct pf_mg_plan {
   pf_mg_desc d;
   int prec;
   float lp_scale[PF_MG_MAX_LEVELS];
-  int ci[PF_MG_MAX_LEVELS];
+  int lb;              // first level solved by the single-CTA bottom kernel (nlev = none)
+  size_t bottom_smem;  // dynamic shared memory of the bottom kernel
   cudaStream_t cap_stream;
   cudaGraphExec_t exec[2];
   size_t exec_nodes[2];
@@ -843,7 +1018,6 @@ int launch_sweep(pf_mg_plan* P, int lv, const T* p_in, bool zero_in, T* p_out, c
   const pf_mg_level& L = P->d.lev[lv];
   SweepArgs<T, TB> a;
   a.n0 = L.nx; a.n1 = L.ny; a.n2 = L.nz;
-  a.ci = P->ci[lv];
   a.p_in = p_in; a.zero_in = zero_in ? 1 : 0; a.p_out = p_out;
   a.b = b; a.b_scale = b_scale;
   a.bx = V.bx; a.by = V.by; a.bz = V.bz;
@@ -856,16 +1030,42 @@ int launch_sweep(pf_mg_plan* P, int lv, const T* p_in, bool zero_in, T* p_out, c
   a.n_total = (int)ncells(L);
   a.mixed = mixed(P) ? 1 : 0;
   a.flux = P->d.stencil == PF_STENCIL_FLUX ? 1 : 0;
-  dim3 grid((L.nz + SW_TK - 1) / SW_TK, (L.ny + SW_TJ - 1) / SW_TJ, (L.nx + a.ci - 1) / a.ci);
-  k_rb_sweep<T, TB><<<grid, SW_NT, 0, s>>>(a);
+  constexpr int TI = 4;
+  dim3 grid((L.nz + SW_TK - 1) / SW_TK, (L.ny + SW_TJ - 1) / SW_TJ, (L.nx + TI - 1) / TI);
+  k_rb_tile<T, TB, TI><<<grid, SW_NT, TileDims<TI>::SMEM, s>>>(a);
   PF_LAUNCHED();
   return PF_OK;
 }
 
-size_t coarsest_smem(const pf_mg_level& L, size_t acc) {
-  const size_t n = (size_t)L.nx * L.ny * L.nz;
-  const size_t nf = (size_t)(L.nx + 1) * L.ny * L.nz + (size_t)L.nx * (L.ny + 1) * L.nz + (size_t)L.nx * L.ny * (L.nz + 1);
-  return n * 3 * acc + nf * sizeof(float);
+template <class T, class TB>
+int launch_bottom(pf_mg_plan* P, const TB* b, const float* b_scale, bool want_mean, cudaStream_t s, T** out) {
+  BottomArgs<T, TB> a;
+  const int lb = P->lb;
+  a.nl = P->d.nlev - lb;
+  for (int l = 0; l < a.nl; ++l) {
+    const pf_mg_level& L = P->d.lev[lb + l];
+    LV<T> V = view<T>(P, lb + l);
+    a.L[l] = BottomLevel{L.nx, L.ny, L.nz, V.bx, V.by, V.bz};
+  }
+  LV<T> V0 = view<T>(P, lb);
+  a.b = b;
+  a.b_scale = b_scale;
+  a.p_out = V0.p0;
+  a.omega = P->d.omega;
+  a.pre = P->d.pre;
+  a.post = P->d.post;
+  a.coarsest = P->d.coarsest;
+  a.rscale = mixed(P) ? 0.125f : 1.f;
+  a.pscale = mixed(P) ? 2.f : 1.f;
+  a.flux = FLUX(P);
+  a.st = ST(P);
+  a.want_mean = want_mean ? 1 : 0;
+  a.mixed = mixed(P) ? 1 : 0;
+  if (mixed(P)) k_bottom<T, TB, double><<<1, BT_NT, P->bottom_smem, s>>>(a);
+  else k_bottom<T, TB, float><<<1, BT_NT, P->bottom_smem, s>>>(a);
+  PF_LAUNCHED();
+  *out = V0.p0;
+  return PF_OK;
 }
 
 #define PF_TRY(x)              \
@@ -883,40 +1083,29 @@ int vcycle(pf_mg_plan* P, int lv, const TB* b, const float* b_scale, bool want_m
   LV<T> V = view<T>(P, lv);
   const int nlev = P->d.nlev;
   const long long n = ncells(L);
+  if (lv == P->lb) return launch_bottom<T, TB>(P, b, b_scale, want_mean, s, out);
   if (lv == nlev - 1) {
-    T* res = V.p0;
-    if (n <= kCoarseMaxCells) {
-      if (mixed(P)) {
-        k_coarsest_b<T, TB, double><<<1, CO_NT, coarsest_smem(L, sizeof(double)), s>>>(
-            L.nx, L.ny, L.nz, b, b_scale, V.bx, V.by, V.bz, res, P->d.coarsest, P->d.omega, ST(P), FLUX(P));
-      } else {
-        k_coarsest_b<T, TB, float><<<1, CO_NT, coarsest_smem(L, sizeof(float)), s>>>(
-            L.nx, L.ny, L.nz, b, b_scale, V.bx, V.by, V.bz, res, P->d.coarsest, P->d.omega, ST(P), FLUX(P));
-      }
-      PF_LAUNCHED();
-    } else {
-      T* cur = nullptr;
-      for (int it = 0; it < P->d.coarsest; ++it) {
-        T* o = (it & 1) ? V.p1 : V.p0;
-        PF_TRY((launch_sweep<T, TB>(P, lv, cur, it == 0, o, b, b_scale, V, nullptr, 1.f, 0, false, true, s)));
-        cur = o;
-      }
-      if (!cur) {
-        PF_CUDA_TRY(cudaMemsetAsync(V.p0, 0, sizeof(T) * n, s));
-        cur = V.p0;
-      }
-      k_mean_of<T><<<red_grid(n), RED_NT, 0, s>>>(n, cur, P->d.partials, CNT(P, CNT_COARSE), ST(P), 0);
-      PF_LAUNCHED();
-      k_shift_mean_inplace<T><<<ew_grid(n), 256, 0, s>>>(n, cur, ST(P));
-      PF_LAUNCHED();
-      res = cur;
+    // coarsest level too large for one CTA: `coarsest` tile sweeps from zero, mean removed
+    T* cur = nullptr;
+    for (int it = 0; it < P->d.coarsest; ++it) {
+      T* o = (it & 1) ? V.p1 : V.p0;
+      PF_TRY((launch_sweep<T, TB>(P, lv, cur, it == 0, o, b, b_scale, V, nullptr, 1.f, 0, false, true, s)));
+      cur = o;
     }
+    if (!cur) {
+      PF_CUDA_TRY(cudaMemsetAsync(V.p0, 0, sizeof(T) * n, s));
+      cur = V.p0;
+    }
+    k_mean_of<T><<<red_grid(n), RED_NT, 0, s>>>(n, cur, P->d.partials, CNT(P, CNT_COARSE), ST(P), 0);
+    PF_LAUNCHED();
+    k_shift_mean_inplace<T><<<ew_grid(n), 256, 0, s>>>(n, cur, ST(P));
+    PF_LAUNCHED();
     if (want_mean) {
-      k_mean_of<T><<<red_grid(n), RED_NT, 0, s>>>(n, res, P->d.partials, CNT(P, CNT_SWEEP_MEAN), ST(P),
+      k_mean_of<T><<<red_grid(n), RED_NT, 0, s>>>(n, cur, P->d.partials, CNT(P, CNT_SWEEP_MEAN), ST(P),
                                                   mixed(P) ? 1 : 0);
       PF_LAUNCHED();
     }
-    *out = res;
+    *out = cur;
     return PF_OK;
   }
   const float rscale = mixed(P) ? 0.125f : 1.f;
@@ -1129,12 +1318,19 @@ template <class T> int precondition_impl(pf_mg_plan* P, const float* r, float* z
   return PF_OK;
 }
 
-template <class T> void set_smem_attrs() {
-  const int mx = 200 * 1024;
-  cudaFuncSetAttribute(k_coarsest_b<T, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_coarsest_b<T, T, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_coarsest_b<T, float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_coarsest_b<T, T, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+template <class T> cudaError_t set_smem_attrs() {
+  const int mx = 220 * 1024, tile = (int)TileDims<4>::SMEM;
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t r) {
+    if (e == cudaSuccess) e = r;
+  };
+  chk(cudaFuncSetAttribute(k_bottom<T, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  chk(cudaFuncSetAttribute(k_bottom<T, T, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  chk(cudaFuncSetAttribute(k_bottom<T, float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  chk(cudaFuncSetAttribute(k_bottom<T, T, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  chk(cudaFuncSetAttribute(k_rb_tile<T, float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile));
+  chk(cudaFuncSetAttribute(k_rb_tile<T, T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile));
+  return e;
 }
 
 }  // namespace
@@ -1174,7 +1370,7 @@ int pf_mg_plan_create(const pf_mg_desc* desc, pf_mg_plan** out) {
       PF_REQUIRE(F.nx == 2 * L.nx && F.ny == 2 * L.ny && F.nz == 2 * L.nz, "level %d is not half of level %d", lv,
                  lv - 1);
     }
-    const long long tiles = (long long)((L.nz + SW_TK - 1) / SW_TK) * ((L.ny + SW_TJ - 1) / SW_TJ);
+    const long long tiles = (long long)((L.nz + SW_TK - 1) / SW_TK) * ((L.ny + SW_TJ - 1) / SW_TJ) * ((L.nx + 3) / 4);
     PF_REQUIRE(tiles <= pf::kPartials, "level %d too large for the sweep reduction", lv);
   }
   pf_mg_plan* P = new pf_mg_plan();
@@ -1184,12 +1380,24 @@ int pf_mg_plan_create(const pf_mg_desc* desc, pf_mg_plan** out) {
   for (int lv = 0; lv < desc->nlev; ++lv) {
     const pf_mg_level& L = desc->lev[lv];
     P->lp_scale[lv] = std::ldexp(desc->coef_scale > 0.f ? desc->coef_scale : 1.f, -2 * lv);
-    const long long tiles = (long long)((L.nz + SW_TK - 1) / SW_TK) * ((L.ny + SW_TJ - 1) / SW_TJ);
-    long long ci = (L.nx * tiles + 443) / 444;
-    if (ci < 4) ci = 4;
-    long long chunks = (L.nx + ci - 1) / ci;
-    while (tiles * chunks > pf::kPartials) { ci *= 2; chunks = (L.nx + ci - 1) / ci; }
-    P->ci[lv] = (int)ci;
+  }
+  // bottom kernel: the deepest run of levels that each fit kBottomMaxCells and
+  // together fit the shared memory of one CTA
+  P->lb = desc->nlev;
+  P->bottom_smem = 0;
+  {
+    size_t floats = 0;
+    const pf_mg_level& Lc = desc->lev[desc->nlev - 1];
+    for (int lv = desc->nlev - 1; lv >= 0; --lv) {
+      const pf_mg_level& L = desc->lev[lv];
+      const long long n = (long long)L.nx * L.ny * L.nz;
+      const size_t f2 = floats + bottom_level_floats(L.nx, L.ny, L.nz);
+      const size_t bytes = f2 * sizeof(float) + 16 + (size_t)Lc.nx * Lc.ny * Lc.nz * sizeof(double);
+      if (n > kBottomMaxCells || bytes > 200 * 1024) break;
+      floats = f2;
+      P->lb = lv;
+      P->bottom_smem = bytes;
+    }
   }
   cudaError_t e = cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&P->h_state[0], sizeof(pf::MGState) * 2, cudaHostAllocDefault);
@@ -1203,9 +1411,14 @@ int pf_mg_plan_create(const pf_mg_desc* desc, pf_mg_plan** out) {
     pf_mg_plan_destroy(P);
     return PF_ERR_CUDA;
   }
-  set_smem_attrs<float>();
-  set_smem_attrs<__half>();
-  set_smem_attrs<__nv_bfloat16>();
+  e = set_smem_attrs<float>();
+  if (e == cudaSuccess) e = set_smem_attrs<__half>();
+  if (e == cudaSuccess) e = set_smem_attrs<__nv_bfloat16>();
+  if (e != cudaSuccess) {
+    pf::set_cuda_error(e, "cudaFuncSetAttribute (shared memory)");
+    pf_mg_plan_destroy(P);
+    return PF_ERR_CUDA;
+  }
   *out = P;
   return PF_OK;
 }

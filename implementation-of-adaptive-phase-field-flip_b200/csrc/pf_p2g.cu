@@ -3,17 +3,21 @@
 // times by pfflip/sim.py:205-228 with one global atomic per weight).
 //
 // Particles are sorted by cell (pf_sort_particles).  One CTA owns a tile of
-// TI x TJ x TK cells and keeps all 8 accumulators (mass and momentum of the 3
-// face grids, cell mass, cell weight sum) of the tile plus a one-node halo in
-// shared memory.  A warp owns one row of TK = 32 cells along k at a time; the
-// row's particles (a contiguous range after the sort) are split evenly over
-// the lanes, so adjacent lanes work on adjacent cells and their shared-memory
-// atomics rarely meet.  After the tile's particles are done, each accumulator
-// node is flushed once with a global reduction (red.global.add.f32); nodes
-// that a rounding edge case puts outside the tile box go to global memory
-// directly.  The weight window and weight of every (particle, node) pair
-// follow the reference exactly: window floor(c - R) + 1 .. floor(c + R)
-// clamped to the grid, w = max(1 - d^2/r^2, 0)^3 (d^2/r^2 as d^2 * (1/r^2)).
+// TI x TJ x 32 cells and the tile's 8 accumulator boxes (tile + one node
+// halo) in shared memory.  A warp owns one row of 32 cells along k and each
+// lane one cell: for each grid the lane sums its particles' weights into a
+// register box covering every node its cell's particles can reach (3x3x3 for
+// the cell grid, 2 along the normal axis of a face grid).  The lanes of a
+// row then combine the k-neighbour parts of their boxes with warp shuffles
+// and add one value per node to shared memory: ~60 shared atomics per cell
+// instead of 64 per particle, and no two lanes of a warp ever add to the same
+// node.  Each tile node is flushed to global memory once (red.global.add).
+//
+// Weights: w = max(1 - d^2/r^2, 0)^3 with d^2 = (fx^2 + fy^2) + fz^2 and
+// fx = (n + o)*dx - x in the reference's order (d^2/r^2 as d^2*(1/r^2)).  The
+// register box includes nodes outside the reference's window
+// floor(c - R) + 1 .. floor(c + R); those lie at least r away, so their
+// weight is exactly 0, and nodes outside the grid are never flushed.
 #include "pf_common.cuh"
 
 namespace pf {
@@ -27,7 +31,7 @@ constexpr size_t PG_SMEM = sizeof(float) * PG_NACC * PG_BOX;
 
 struct P2GArgs {
   int nx, ny, nz;
-  float dx, inv_r2, R;
+  float dx, inv_r2;
   float rho_l, rho_g;
   const float4* pos;
   const float4* vel;
@@ -35,9 +39,123 @@ struct P2GArgs {
   float* out[PG_NACC];  // mass x,y,z, mom x,y,z, cell_mass, cell_wsum
 };
 
-__device__ __forceinline__ float splat_w(float d2, float inv_r2) {
-  float t = fmaxf(1.f - d2 * inv_r2, 0.f);
-  return t * t * t;
+// Register box of grid G (0,1,2 = face axis, 3 = cell centres) for one cell.
+template <int G> struct Box {
+  static constexpr int NX = (G == 0) ? 2 : 3, NY = (G == 1) ? 2 : 3, NZ = (G == 2) ? 2 : 3;
+  static constexpr int LX = (G == 0) ? 0 : -1, LY = (G == 1) ? 0 : -1, LZ = (G == 2) ? 0 : -1;
+  static constexpr float OX = (G == 0) ? 0.f : 0.5f, OY = (G == 1) ? 0.f : 0.5f, OZ = (G == 2) ? 0.f : 0.5f;
+  float m[NX][NY][NZ];   // sum of w * m_p
+  float q[NX][NY][NZ];   // sum of w * m_p * u_G (faces) or of w (cells)
+
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int a = 0; a < NX; ++a)
+#pragma unroll
+      for (int b = 0; b < NY; ++b)
+#pragma unroll
+        for (int c = 0; c < NZ; ++c) m[a][b][c] = q[a][b][c] = 0.f;
+  }
+
+  // add one particle (x, mass, velocity component) of cell (ci, cj, ck)
+  __device__ __forceinline__ void add(int ci, int cj, int ck, const float x[3], float mp, float up, float dx,
+                                      float inv_r2) {
+    float DX[NX], DY[NY], DZ[NZ];
+#pragma unroll
+    for (int a = 0; a < NX; ++a) {
+      const float f = ((float)(ci + LX + a) + OX) * dx - x[0];
+      DX[a] = f * f;
+    }
+#pragma unroll
+    for (int b = 0; b < NY; ++b) {
+      const float f = ((float)(cj + LY + b) + OY) * dx - x[1];
+      DY[b] = f * f;
+    }
+#pragma unroll
+    for (int c = 0; c < NZ; ++c) {
+      const float f = ((float)(ck + LZ + c) + OZ) * dx - x[2];
+      DZ[c] = f * f;
+    }
+#pragma unroll
+    for (int a = 0; a < NX; ++a)
+#pragma unroll
+      for (int b = 0; b < NY; ++b) {
+        const float dxy = DX[a] + DY[b];
+#pragma unroll
+        for (int c = 0; c < NZ; ++c) {
+          const float t = fmaxf(1.f - (dxy + DZ[c]) * inv_r2, 0.f);
+          const float w = t * t * t;
+          const float wm = w * mp;
+          m[a][b][c] += wm;
+          q[a][b][c] += (G < 3) ? wm * up : w;
+        }
+      }
+  }
+
+  // combine along k across the lanes of the row and add to the shared boxes.
+  // Lane l owns cell k0 + l; box k index of node k is k - k0 - LZ.
+  __device__ __forceinline__ void flush(float* sm1, float* sm2, int li, int lj, int lane) {
+#pragma unroll
+    for (int a = 0; a < NX; ++a)
+#pragma unroll
+      for (int b = 0; b < NY; ++b) {
+        const int row = ((li + a) * PG_BJ + (lj + b)) * PG_BK;
+        if (NZ == 3) {
+          // node k0+l (box index l+1) = own centre + lane l-1's upper + lane l+1's lower
+          const float up1 = __shfl_up_sync(0xffffffffu, m[a][b][2], 1);
+          const float up2 = __shfl_up_sync(0xffffffffu, q[a][b][2], 1);
+          const float dn1 = __shfl_down_sync(0xffffffffu, m[a][b][0], 1);
+          const float dn2 = __shfl_down_sync(0xffffffffu, q[a][b][0], 1);
+          float v1 = m[a][b][1], v2 = q[a][b][1];
+          if (lane > 0) { v1 += up1; v2 += up2; }
+          if (lane < 31) { v1 += dn1; v2 += dn2; }
+          if (v1 != 0.f) atomicAdd(sm1 + row + lane + 1, v1);
+          if (v2 != 0.f) atomicAdd(sm2 + row + lane + 1, v2);
+          if (lane == 0) {
+            if (m[a][b][0] != 0.f) atomicAdd(sm1 + row, m[a][b][0]);
+            if (q[a][b][0] != 0.f) atomicAdd(sm2 + row, q[a][b][0]);
+          }
+          if (lane == 31) {
+            if (m[a][b][2] != 0.f) atomicAdd(sm1 + row + 33, m[a][b][2]);
+            if (q[a][b][2] != 0.f) atomicAdd(sm2 + row + 33, q[a][b][2]);
+          }
+        } else {
+          // z-faces: node k0+l (box index l) = own lower + lane l-1's upper
+          const float up1 = __shfl_up_sync(0xffffffffu, m[a][b][NZ - 1], 1);
+          const float up2 = __shfl_up_sync(0xffffffffu, q[a][b][NZ - 1], 1);
+          float v1 = m[a][b][0], v2 = q[a][b][0];
+          if (lane > 0) { v1 += up1; v2 += up2; }
+          if (v1 != 0.f) atomicAdd(sm1 + row + lane, v1);
+          if (v2 != 0.f) atomicAdd(sm2 + row + lane, v2);
+          if (lane == 31) {
+            if (m[a][b][NZ - 1] != 0.f) atomicAdd(sm1 + row + 32, m[a][b][NZ - 1]);
+            if (q[a][b][NZ - 1] != 0.f) atomicAdd(sm2 + row + 32, q[a][b][NZ - 1]);
+          }
+        }
+      }
+  }
+};
+
+// one grid over the particles of cell (i, j, k) (range [s, e)), then the row flush
+template <int G>
+__device__ __forceinline__ void p2g_grid(const P2GArgs& a, float* acc, int i, int j, int k, int s, int e, int li,
+                                         int lj, int lane) {
+  Box<G> box;
+  box.zero();
+  for (int t = s; t < e; ++t) {
+    const float4 P = __ldg(a.pos + t);
+    const int flags = __float_as_int(P.w);
+    if ((flags >> PF_PSTATE_SHIFT) & 3) continue;  // droplets / dead particles do not splat
+    const float mp = (flags & PF_FLAG_LIQUID) ? a.rho_l : a.rho_g;
+    float up = 0.f;
+    if (G < 3) {
+      const float4 V = __ldg(a.vel + t);
+      up = G == 0 ? V.x : G == 1 ? V.y : V.z;
+    }
+    const float x[3] = {P.x, P.y, P.z};
+    box.add(i, j, k, x, mp, up, a.dx, a.inv_r2);
+  }
+  const int a1 = (G < 3) ? G : 6, a2 = (G < 3) ? 3 + G : 7;
+  box.flush(acc + a1 * PG_BOX, acc + a2 * PG_BOX, li, lj, lane);
 }
 
 __global__ void __launch_bounds__(PG_NT) k_p2g(P2GArgs a) {
@@ -48,83 +166,23 @@ __global__ void __launch_bounds__(PG_NT) k_p2g(P2GArgs a) {
   __syncthreads();
 
   const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const float dx = a.dx, R = a.R, inv_r2 = a.inv_r2;
-  const int k1 = min(k0 + PG_TK, nz);
-
   for (int row = warp; row < PG_TI * PG_TJ; row += PG_NT / 32) {
-    const int i = i0 + row / PG_TJ, j = j0 + row % PG_TJ;
-    if (i >= nx || j >= ny || k0 >= nz) continue;
-    const int key0 = (i * ny + j) * nz + k0;
-    const int rs = a.cell_start[key0], re = a.cell_start[key0 + (k1 - k0)];
-    const int len = re - rs;
-    const int chunk = (len + 31) >> 5;
-    const int ps = rs + lane * chunk, pe = min(re, ps + chunk);
-    for (int t = ps; t < pe; ++t) {
-      const float4 P = __ldg(a.pos + t);
-      const int flags = __float_as_int(P.w);
-      if ((flags >> PF_PSTATE_SHIFT) & 3) continue;  // droplets / dead particles do not splat
-      const float4 V = __ldg(a.vel + t);
-      const float m = (flags & PF_FLAG_LIQUID) ? a.rho_l : a.rho_g;
-      const float q[3] = {P.x / dx, P.y / dx, P.z / dx};
-      const float xp[3] = {P.x, P.y, P.z};
-      const float up[3] = {V.x, V.y, V.z};
-#pragma unroll
-      for (int g = 0; g < 4; ++g) {
-        // node offsets o_d and grid extents of grid g (3 = cell centres)
-        float o[3];
-        int n[3], blo[3];
-        const int tile0[3] = {i0, j0, k0};
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const bool normal = (g == d);
-          o[d] = normal ? 0.f : 0.5f;
-          n[d] = (d == 0 ? nx : d == 1 ? ny : nz) + (normal ? 1 : 0);
-          blo[d] = tile0[d] - (normal ? 0 : 1);
-        }
-        int lo[3], hi[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const float c = q[d] - o[d];
-          lo[d] = max((int)floorf(c - R) + 1, 0);
-          hi[d] = min((int)floorf(c + R), n[d] - 1);
-        }
-        const float v1 = m;
-        const float v2 = (g < 3) ? up[g] : 0.f;
-        float* A1 = acc + (g < 3 ? g : 6) * PG_BOX;
-        float* A2 = acc + (g < 3 ? 3 + g : 7) * PG_BOX;
-        float* G1 = a.out[g < 3 ? g : 6];
-        float* G2 = a.out[g < 3 ? 3 + g : 7];
-        for (int ii = lo[0]; ii <= hi[0]; ++ii) {
-          const float fx = ((float)ii + o[0]) * dx - xp[0];
-          for (int jj = lo[1]; jj <= hi[1]; ++jj) {
-            const float fy = ((float)jj + o[1]) * dx - xp[1];
-            const float fxy = fx * fx + fy * fy;
-            for (int kk = lo[2]; kk <= hi[2]; ++kk) {
-              const float fz = ((float)kk + o[2]) * dx - xp[2];
-              const float w = splat_w(fxy + fz * fz, inv_r2);
-              if (w > 0.f) {
-                const float wm = w * v1;
-                const float w2 = (g < 3) ? wm * v2 : w;
-                const int li = ii - blo[0], lj = jj - blo[1], lk = kk - blo[2];
-                if ((unsigned)li < (unsigned)PG_BI && (unsigned)lj < (unsigned)PG_BJ &&
-                    (unsigned)lk < (unsigned)PG_BK) {
-                  const int e = (li * PG_BJ + lj) * PG_BK + lk;
-                  atomicAdd(A1 + e, wm);
-                  atomicAdd(A2 + e, w2);
-                } else {
-                  const long long ge = ((long long)ii * n[1] + jj) * n[2] + kk;
-                  atomicAdd(G1 + ge, wm);
-                  atomicAdd(G2 + ge, w2);
-                }
-              }
-            }
-          }
-        }
-      }
+    const int li = row / PG_TJ, lj = row % PG_TJ;
+    const int i = i0 + li, j = j0 + lj, k = k0 + lane;
+    if (i >= nx || j >= ny) continue;  // warp-uniform
+    int s = 0, e = 0;
+    if (k < nz) {
+      const int key = (i * ny + j) * nz + k;
+      s = a.cell_start[key];
+      e = a.cell_start[key + 1];
     }
+    p2g_grid<3>(a, acc, i, j, k, s, e, li, lj, lane);
+    p2g_grid<0>(a, acc, i, j, k, s, e, li, lj, lane);
+    p2g_grid<1>(a, acc, i, j, k, s, e, li, lj, lane);
+    p2g_grid<2>(a, acc, i, j, k, s, e, li, lj, lane);
   }
   __syncthreads();
-  // flush: each node once
+  // flush: each tile node once
   for (int e = tid; e < PG_NACC * PG_BOX; e += PG_NT) {
     const float v = acc[e];
     if (v == 0.f) continue;
@@ -150,7 +208,10 @@ extern "C" int pf_p2g(const pf_grid* g, int64_t n, const float* pos4, const floa
   PF_REQUIRE(g && pos4 && vel4 && cell_start && mass_x && mass_y && mass_z && mom_x && mom_y && mom_z && cell_mass &&
                  cell_wsum,
              "null argument");
-  PF_REQUIRE(g->nx > 0 && g->ny > 0 && g->nz > 0 && g->dx > 0.f && r_p > 0.f, "bad grid");
+  PF_REQUIRE(g->nx > 0 && g->ny > 0 && g->nz > 0 && g->dx > 0.f, "bad grid");
+  // the register boxes cover nodes within one cell of the particle's cell: the
+  // support radius must not exceed one cell (the reference uses r_p = dx)
+  PF_REQUIRE(r_p > 0.f && r_p <= g->dx, "r_p must be in (0, dx]");
   PF_REQUIRE(aligned16(pos4) && aligned16(vel4), "particle streams must be 16-byte aligned");
   static bool attr_set = false;
   if (!attr_set) {
@@ -168,7 +229,6 @@ extern "C" int pf_p2g(const pf_grid* g, int64_t n, const float* pos4, const floa
   P2GArgs a;
   a.nx = nx; a.ny = ny; a.nz = nz;
   a.dx = g->dx;
-  a.R = r_p / g->dx;
   a.inv_r2 = 1.f / (r_p * r_p);
   a.rho_l = rho_l; a.rho_g = rho_g;
   a.pos = reinterpret_cast<const float4*>(pos4);

@@ -172,6 +172,7 @@ class Simulator:
         self.step_index = 0
         self.stats: list[dict] = []
         self._warned_droplets = False
+        self._marks = None  # per-stage CUDA events when stage timing is on
 
         self.px = ParticleField(self, "pos")
         self.pv = ParticleField(self, "vel")
@@ -186,32 +187,55 @@ class Simulator:
         self.solid.assign(np.ascontiguousarray(mask, np.int32))
         self.has_solids = bool(np.any(mask))
 
-    def set_particles(self, pos: np.ndarray, vel: np.ndarray, ptype: np.ndarray):
-        """Upload particles (NumPy (n,3) positions and velocities, (n,) types)."""
-        pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
-        vel = np.ascontiguousarray(vel, np.float32).reshape(-1, 3)
-        ptype = np.ascontiguousarray(ptype).reshape(-1)
-        n = len(pos)
-        if len(vel) != n or len(ptype) != n:
+    def set_particles(self, pos, vel, ptype):
+        """Upload particles: (n,3) positions and velocities, (n,) types (0 air,
+        1 liquid), as NumPy arrays or host/device torch tensors.  Buffers are
+        reused when the particle count is unchanged."""
+        t = lambda a, dt: (a if isinstance(a, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(a))).to(dt)  # noqa: E731
+        pos = t(pos, torch.float32).reshape(-1, 3)
+        vel = t(vel, torch.float32).reshape(-1, 3)
+        ptype = t(ptype, torch.int32).reshape(-1)
+        n = pos.shape[0]
+        if vel.shape[0] != n or ptype.shape[0] != n:
             raise ValueError("pos, vel and ptype must have the same length")
-        self.n_particles = n
         dev = self.dev
-        p4 = torch.empty((n, 4), dtype=torch.float32, device=dev)
-        v4 = torch.empty((n, 4), dtype=torch.float32, device=dev)
-        p4[:, :3] = torch.from_numpy(pos).to(dev)
-        v4[:, :3] = torch.from_numpy(vel).to(dev)
-        p4.view(torch.int32)[:, 3] = torch.from_numpy((ptype == 1).astype(np.int32)).to(dev)
+        if self._pos4 is None or self.n_particles != n:
+            self._alloc_particles(n)
+        self.n_particles = n
+        p4, v4 = self._pos4, self._vel4
+        p4[:, :3].copy_(pos, non_blocking=True)
+        v4[:, :3].copy_(vel, non_blocking=True)
+        p4.view(torch.int32)[:, 3].copy_((ptype == 1).to(torch.int32), non_blocking=True)
         v4.view(torch.int32)[:, 3] = torch.arange(n, dtype=torch.int32, device=dev)
-        self._pos4, self._vel4 = p4, v4
-        self._pos4_alt = torch.empty_like(p4)
-        self._vel4_alt = torch.empty_like(v4)
+        self._sort()
+
+    def read_particles(self, pos_out=None, vel_out=None):
+        """Positions and velocities in the original order, copied into the given
+        (pinned) host tensors when provided; returns (pos, vel)."""
+        ids = self._ids().long()
+        out = []
+        for src, dst in ((self._pos4, pos_out), (self._vel4, vel_out)):
+            tmp = torch.empty((self.n_particles, 3), dtype=torch.float32, device=self.dev)
+            tmp[ids] = src[:, :3]
+            if dst is None:
+                out.append(tmp.cpu())
+            else:
+                dst.copy_(tmp, non_blocking=True)
+                out.append(dst)
+        return tuple(out)
+
+    def _alloc_particles(self, n):
+        dev = self.dev
+        self._pos4 = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        self._vel4 = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        self._pos4_alt = torch.empty_like(self._pos4)
+        self._vel4_alt = torch.empty_like(self._vel4)
         self._keys = torch.empty(n, dtype=torch.int32, device=dev)
         self._perm = torch.empty(n, dtype=torch.int32, device=dev)
         nc = self.res[0] * self.res[1] * self.res[2]
         self._cell_start = torch.zeros(nc + 1, dtype=torch.int32, device=dev)
         wsb = int(N.lib().pf_sort_workspace_bytes(C.byref(self._g), n))
         self._sort_ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
-        self._sort()
 
     def _ids(self):
         return self._vel4.view(torch.int32)[:, 3]
@@ -229,6 +253,31 @@ class Simulator:
         self._pos4, self._pos4_alt = self._pos4_alt, self._pos4
         self._vel4, self._vel4_alt = self._vel4_alt, self._vel4
 
+    # ------------------------------------------------------------------ timing
+    def enable_stage_timing(self, on: bool = True):
+        """Record a CUDA event at every stage boundary of ``step`` (no syncs)."""
+        self._marks = [] if on else None
+
+    def _mark(self, name):
+        if self._marks is not None:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record()
+            self._marks.append((name, e))
+
+    def stage_times(self, reset=True):
+        """Per-stage device time over the recorded steps: {stage: (launches, total_ms)}."""
+        torch.cuda.synchronize(self.dev)
+        out = {}
+        m = self._marks or []
+        for (name, e0), (_, e1) in zip(m[:-1], m[1:]):
+            if name == "<end>":
+                continue
+            c, t = out.get(name, (0, 0.0))
+            out[name] = (c + 1, t + e0.elapsed_time(e1))
+        if reset and self._marks is not None:
+            self._marks = []
+        return out
+
     # ------------------------------------------------------------------ step
     def dt_from_cfl(self) -> float:
         cfg = self.cfg
@@ -243,15 +292,23 @@ class Simulator:
         if dt is None:
             dt = self.dt_from_cfl()
         t0 = time.perf_counter()
-        self._p2g()
+        mark = self._mark
+        self._p2g(mark=mark)
+        mark("phase_beta")
         self._phase_field_and_coefficients()
+        mark("forces")
         self._add_forces(dt, save_vel_star=True)
-        pcg_it, pcg_res = self._pressure_solve(dt, verbose=verbose)
+        pcg_it, pcg_res = self._pressure_solve(dt, verbose=verbose, mark=mark)
+        mark("project")
         self._project(dt)
+        mark("divergence")
         self._divergence_async()
+        mark("extrapolate")
         self._extrapolate_liquid_velocity()
         self._droplets(dt)
+        mark("g2p_advect")
         self._g2p_advect(dt, do_g2p=True, do_advect=True)
+        mark("<end>")
         div_after = float(self._scal[1].item())  # synchronises the stream
         wall = time.perf_counter() - t0
         self.time += dt
@@ -270,10 +327,14 @@ class Simulator:
         return rec
 
     # ------------------------------------------------------------------ stages
-    def _p2g(self):
+    def _p2g(self, mark=None):
         """Sort, then eq. (3)-(6) splatting to faces and cells (pfflip/sim.py:205-236)."""
         cfg = self.cfg
+        if mark:
+            mark("sort")
         self._sort()
+        if mark:
+            mark("p2g")
         N.call("pf_p2g", C.byref(self._g), self.n_particles, self._pos4.data_ptr(), self._vel4.data_ptr(),
                self._cell_start.data_ptr(), float(cfg.rho_l), float(cfg.rho_g), float(np.float32(cfg.r_p)),
                *(N.ptr(a) for a in self.mass), *(N.ptr(a) for a in self.mom), N.ptr(self.cell_mass),
@@ -297,11 +358,17 @@ class Simulator:
                N.ptr(self.solid) if self.has_solids else None, float(g[0]), float(g[1]), float(g[2]), float(dt),
                N.stream())
 
-    def _pressure_solve(self, dt: float, verbose: bool = False):
+    def _pressure_solve(self, dt: float, verbose: bool = False, mark=None):
         cfg = self.cfg
+        if mark:
+            mark("rhs")
         N.call("pf_build_rhs", C.byref(self._g), *(N.ptr(a) for a in self.vel), N.ptr(self.cell_wsum),
                N.ptr(self.rhs), float(dt), float(self.rho_tilde_0), float(cfg.k_div), N.stream())
+        if mark:
+            mark("hierarchy")
         self.solver.build_hierarchy(*self.beta)
+        if mark:
+            mark("solve")
         return self.solver.solve(self.rhs, self.pressure, tol=cfg.pcg_tol, max_iter=cfg.pcg_max_iter,
                                  verbose=verbose)
 
