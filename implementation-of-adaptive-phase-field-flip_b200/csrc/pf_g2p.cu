@@ -8,6 +8,8 @@
 // RK3 trace through the extrapolated (liquid) or raw (air) field, the clamp
 // and the wall reflection.  u - u* is formed per interpolation tap, which is
 // the reference's interpolation of the difference field, value for value.
+// Interpolation coordinates are x * (1/dx): identical to the reference's x/dx
+// for power-of-two dx, within an ulp otherwise.
 // Particles are in cell order, so neighbouring threads gather neighbouring
 // taps from L1/L2.
 #include "pf_common.cuh"
@@ -17,7 +19,7 @@ namespace pf {
 struct G2PArgs {
   long long n;
   int nx, ny, nz;
-  float dx, dt, a_liq, a_air;
+  float dx, inv_dx, dt, a_liq, a_air;
   float lo[3], hi[3];
   float4* pos;
   float4* vel;
@@ -28,45 +30,67 @@ struct G2PArgs {
   int do_g2p, do_advect;
 };
 
-// clamped trilinear sample of face grid `c` (pfflip/kernels.py:52-79); q = x/dx.
-// DIFF: samples f - fs tap by tap.
-template <bool DIFF>
-__device__ __forceinline__ float sample_face(const float* __restrict__ f, const float* __restrict__ fs, int c,
-                                             const float q[3], int nx, int ny, int nz) {
-  const int n0 = nx + (c == 0), n1 = ny + (c == 1), n2 = nz + (c == 2);
-  const float g0 = q[0] - (c == 0 ? 0.f : 0.5f);
-  const float g1 = q[1] - (c == 1 ? 0.f : 0.5f);
-  const float g2 = q[2] - (c == 2 ? 0.f : 0.5f);
-  const int i0 = (int)floorf(g0), j0 = (int)floorf(g1), k0 = (int)floorf(g2);
-  const float tx = g0 - (float)i0, ty = g1 - (float)j0, tz = g2 - (float)k0;
-  float acc = 0.f;
+// Per-position interpolation frame: for each axis d and node offset o in
+// {0, 0.5}, the clamped lower/upper tap indices and the upper weight of
+// g = x/dx - o (pfflip/kernels.py:52-79).  Face grid c uses offset 0 on axis c
+// and 0.5 on the other axes, so all three components share one frame.
+struct Frame {
+  int lo[3][2], hi[3][2];
+  float t[3][2];
+};
+
+__device__ __forceinline__ void make_frame(const float x[3], float inv_dx, int nx, int ny, int nz, Frame& f) {
+  const int n[3] = {nx, ny, nz};
 #pragma unroll
-  for (int di = 0; di < 2; ++di) {
-    const float wi = di == 0 ? 1.f - tx : tx;
-    const int ii = min(max(i0 + di, 0), n0 - 1);
+  for (int d = 0; d < 3; ++d) {
+    const float q = x[d] * inv_dx;
 #pragma unroll
-    for (int dj = 0; dj < 2; ++dj) {
-      const float wj = dj == 0 ? 1.f - ty : ty;
-      const int jj = min(max(j0 + dj, 0), n1 - 1);
-      const long long row = ((long long)ii * n1 + jj) * n2;
-#pragma unroll
-      for (int dk = 0; dk < 2; ++dk) {
-        const float wk = dk == 0 ? 1.f - tz : tz;
-        const int kk = min(max(k0 + dk, 0), n2 - 1);
-        float v = __ldg(f + row + kk);
-        if (DIFF) v = v - __ldg(fs + row + kk);
-        acc += wi * wj * wk * v;
-      }
+    for (int v = 0; v < 2; ++v) {
+      // v = 0: offset 0 (normal axis, extent n+1); v = 1: offset 0.5 (extent n)
+      const float g = v == 0 ? q : q - 0.5f;
+      const int i0 = (int)floorf(g);
+      const int last = v == 0 ? n[d] : n[d] - 1;
+      f.t[d][v] = g - (float)i0;
+      f.lo[d][v] = min(max(i0, 0), last);
+      f.hi[d][v] = min(max(i0 + 1, 0), last);
     }
   }
+}
+
+// trilinear sample of face grid c (DIFF: of f - fs, tap by tap), taps and sums
+// in the reference's order
+template <bool DIFF>
+__device__ __forceinline__ float sample_c(const float* __restrict__ f, const float* __restrict__ fs, int c,
+                                          const Frame& fr, int ny, int nz) {
+  const int vi = c == 0 ? 0 : 1, vj = c == 1 ? 0 : 1, vk = c == 2 ? 0 : 1;
+  const int n1 = ny + (c == 1), n2 = nz + (c == 2);
+  const float tx = fr.t[0][vi], ty = fr.t[1][vj], tz = fr.t[2][vk];
+  const int I[2] = {fr.lo[0][vi], fr.hi[0][vi]}, J[2] = {fr.lo[1][vj], fr.hi[1][vj]};
+  const int K[2] = {fr.lo[2][vk], fr.hi[2][vk]};
+  const float wi[2] = {1.f - tx, tx}, wj[2] = {1.f - ty, ty}, wk[2] = {1.f - tz, tz};
+  float acc = 0.f;
+#pragma unroll
+  for (int di = 0; di < 2; ++di)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj) {
+      const long long row = ((long long)I[di] * n1 + J[dj]) * n2;
+      const float wij = wi[di] * wj[dj];
+#pragma unroll
+      for (int dk = 0; dk < 2; ++dk) {
+        float v = __ldg(f + row + K[dk]);
+        if (DIFF) v = v - __ldg(fs + row + K[dk]);
+        acc += wij * wk[dk] * v;
+      }
+    }
   return acc;
 }
 
-__device__ __forceinline__ void sample_vel(const float* const f[3], const float x[3], float dx, int nx, int ny, int nz,
-                                           float out[3]) {
-  const float q[3] = {x[0] / dx, x[1] / dx, x[2] / dx};
+__device__ __forceinline__ void sample_vel(const float* const f[3], const float x[3], float inv_dx, int nx, int ny,
+                                           int nz, float out[3]) {
+  Frame fr;
+  make_frame(x, inv_dx, nx, ny, nz, fr);
 #pragma unroll
-  for (int c = 0; c < 3; ++c) out[c] = sample_face<false>(f[c], nullptr, c, q, nx, ny, nz);
+  for (int c = 0; c < 3; ++c) out[c] = sample_c<false>(f[c], nullptr, c, fr, ny, nz);
 }
 
 __global__ void __launch_bounds__(256) k_g2p_advect(G2PArgs a) {
@@ -80,11 +104,12 @@ __global__ void __launch_bounds__(256) k_g2p_advect(G2PArgs a) {
     float v[3] = {V.x, V.y, V.z};
     if (a.do_g2p && pstate == 0) {
       const float alpha = liquid ? a.a_liq : a.a_air;
-      const float q[3] = {x[0] / a.dx, x[1] / a.dx, x[2] / a.dx};
+      Frame fr;
+      make_frame(x, a.inv_dx, a.nx, a.ny, a.nz, fr);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const float delta = sample_face<true>(a.u[c], a.us[c], c, q, a.nx, a.ny, a.nz);
-        const float pic = sample_face<false>(a.u[c], nullptr, c, q, a.nx, a.ny, a.nz);
+        const float delta = sample_c<true>(a.u[c], a.us[c], c, fr, a.ny, a.nz);
+        const float pic = sample_c<false>(a.u[c], nullptr, c, fr, a.ny, a.nz);
         v[c] = alpha * (v[c] + delta) + (1.f - alpha) * pic;
       }
     }
@@ -92,14 +117,14 @@ __global__ void __launch_bounds__(256) k_g2p_advect(G2PArgs a) {
       if (pstate == 0) {
         const float* const* f = liquid ? a.ul : a.u;
         float k1[3], k2[3], k3[3], y[3];
-        sample_vel(f, x, a.dx, a.nx, a.ny, a.nz, k1);
+        sample_vel(f, x, a.inv_dx, a.nx, a.ny, a.nz, k1);
         const float h1 = 0.5f * a.dt, h2 = 0.75f * a.dt;
 #pragma unroll
         for (int c = 0; c < 3; ++c) y[c] = x[c] + h1 * k1[c];
-        sample_vel(f, y, a.dx, a.nx, a.ny, a.nz, k2);
+        sample_vel(f, y, a.inv_dx, a.nx, a.ny, a.nz, k2);
 #pragma unroll
         for (int c = 0; c < 3; ++c) y[c] = x[c] + h2 * k2[c];
-        sample_vel(f, y, a.dx, a.nx, a.ny, a.nz, k3);
+        sample_vel(f, y, a.inv_dx, a.nx, a.ny, a.nz, k3);
         const float c1 = 2.0f / 9.0f, c2 = 3.0f / 9.0f, c3 = 4.0f / 9.0f;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -176,7 +201,9 @@ extern "C" int pf_g2p_advect(const pf_grid* g, int64_t n, float* pos4, float* ve
   G2PArgs a;
   a.n = n;
   a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
-  a.dx = g->dx; a.dt = dt;
+  a.dx = g->dx;
+  a.inv_dx = (float)(1.0 / (double)g->dx);  // exact for the power-of-two spacings of the benchmarks
+  a.dt = dt;
   a.a_liq = alpha_liquid; a.a_air = alpha_air;
   for (int c = 0; c < 3; ++c) {
     a.lo[c] = lo ? lo[c] : 0.f;

@@ -24,7 +24,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
+
+#include <cuda.h>
 
 #include "pf_common.cuh"
 
@@ -44,7 +47,7 @@ struct MGState {
 };
 static_assert(sizeof(MGState) <= PF_MG_STATE_BYTES, "state size");
 
-enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_BREAKDOWN = 2, ST_NONFINITE = 3, ST_ZERO_RHS = 4 };
+enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_BREAKDOWN = 2, ST_NONFINITE = 3, ST_ZERO_RHS = 4, ST_TMA_TIMEOUT = 5 };
 
 // counters used by the last-CTA reductions (one per call site so that two
 // reductions in flight never share a ticket)
@@ -115,11 +118,18 @@ __global__ void k_apply_A(int nx, int ny, int nz, const float* __restrict__ p, c
 template <class T>
 __global__ void k_level_coefs(int nx, int ny, int nz, const float* __restrict__ bx, const float* __restrict__ by,
                               const float* __restrict__ bz, float* __restrict__ diag, T* bx_lp, T* by_lp, T* bz_lp,
-                              float lp_scale) {
-  // diag (pfflip/poisson.py:41-51) and, in 16-bit mode, the scaled copies
+                              float lp_scale, float* __restrict__ bz_pad, int bz_pitch) {
+  // diag (pfflip/poisson.py:41-51), the row-padded z-faces for TMA and, in
+  // 16-bit mode, the scaled copies
   const long long nc = (long long)nx * ny * nz;
   const long long nfx = (long long)(nx + 1) * ny * nz, nfy = (long long)nx * (ny + 1) * nz,
                   nfz = (long long)nx * ny * (nz + 1);
+  if (bz_pad) {
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nfz; f += (long long)gridDim.x * blockDim.x) {
+      const long long row = f / (nz + 1);
+      bz_pad[row * bz_pitch + (f - row * (nz + 1))] = bz[f];
+    }
+  }
   const long long tot = nc + (bx_lp ? nfx + nfy + nfz : 0);
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
        e += (long long)gridDim.x * blockDim.x) {
@@ -266,42 +276,72 @@ __global__ void __launch_bounds__(SW_NT) k_rb_tile(SweepArgs<T, TB> a) {
   const float bsc = a.b_scale ? *a.b_scale : 1.f;
   const int hn1 = n1 >> 1, hn2 = n2 >> 1;
 
-  // ---- loads (zero outside the level)
-  for (int e = tid; e < D::PN; e += SW_NT) {
+  // ---- loads (zero outside the level): every load of the CTA is issued into
+  // registers before any is stored, so they are all in flight together
+  constexpr int IP = (D::PN + SW_NT - 1) / SW_NT, IB = (D::CN + SW_NT - 1) / SW_NT;
+  constexpr int IX = (D::XN + SW_NT - 1) / SW_NT, IY = (D::YN + SW_NT - 1) / SW_NT;
+  constexpr int IZ = (D::ZN + SW_NT - 1) / SW_NT;
+  float vp[IP], vb[IB], vx[IX], vy[IY], vz[IZ];
+#pragma unroll
+  for (int u = 0; u < IP; ++u) {
+    const int e = tid + u * SW_NT;
     const int c = e % D::PK, t = e / D::PK, r = t % D::PJ, q = t / D::PJ;
     const int i = i0 - 2 + q, j = j0 - 2 + r, k = k0 - 2 + c;
     float v = 0.f;
-    if (i >= 0 && i < n0 && j >= 0 && j < n1 && k >= 0 && k < n2) {
+    if (e < D::PN && i >= 0 && i < n0 && j >= 0 && j < n1 && k >= 0 && k < n2) {
       const long long g = i * sI + (long long)j * n2 + k;
       if (!a.zero_in) v = ldT(a.p_in + g);
       if (a.pc) v += ldT(a.pc + ((long long)(i >> 1) * hn1 + (j >> 1)) * hn2 + (k >> 1)) * a.pc_scale;
     }
-    sP[e] = v;
+    vp[u] = v;
   }
-  for (int e = tid; e < D::CN; e += SW_NT) {
+#pragma unroll
+  for (int u = 0; u < IB; ++u) {
+    const int e = tid + u * SW_NT;
     const int c = e % D::CK, t = e / D::CK, r = t % D::CJ, q = t / D::CJ;
     const int i = i0 - 1 + q, j = j0 - 1 + r, k = k0 - 1 + c;
-    const bool in = i >= 0 && i < n0 && j >= 0 && j < n1 && k >= 0 && k < n2;
-    sB[e] = in ? ldT(a.b + i * sI + (long long)j * n2 + k) * bsc : 0.f;
+    const bool in = e < D::CN && i >= 0 && i < n0 && j >= 0 && j < n1 && k >= 0 && k < n2;
+    vb[u] = in ? ldT(a.b + i * sI + (long long)j * n2 + k) * bsc : 0.f;
   }
-  for (int e = tid; e < D::XN; e += SW_NT) {  // x-faces i0-1 .. i0+TI+1
+#pragma unroll
+  for (int u = 0; u < IX; ++u) {  // x-faces i0-1 .. i0+TI+1
+    const int e = tid + u * SW_NT;
     const int c = e % D::CK, t = e / D::CK, r = t % D::CJ, q = t / D::CJ;
     const int f = i0 - 1 + q, j = j0 - 1 + r, k = k0 - 1 + c;
-    const bool in = f >= 0 && f <= n0 && j >= 0 && j < n1 && k >= 0 && k < n2;
-    sX[e] = in ? ldT(a.bx + (long long)f * sI + (long long)j * n2 + k) : 0.f;
+    const bool in = e < D::XN && f >= 0 && f <= n0 && j >= 0 && j < n1 && k >= 0 && k < n2;
+    vx[u] = in ? ldT(a.bx + (long long)f * sI + (long long)j * n2 + k) : 0.f;
   }
-  for (int e = tid; e < D::YN; e += SW_NT) {  // y-faces j0-1 .. j0+TJ+1
+#pragma unroll
+  for (int u = 0; u < IY; ++u) {  // y-faces j0-1 .. j0+TJ+1
+    const int e = tid + u * SW_NT;
     const int c = e % D::CK, t = e / D::CK, r = t % (D::CJ + 1), q = t / (D::CJ + 1);
     const int i = i0 - 1 + q, f = j0 - 1 + r, k = k0 - 1 + c;
-    const bool in = i >= 0 && i < n0 && f >= 0 && f <= n1 && k >= 0 && k < n2;
-    sY[e] = in ? ldT(a.by + ((long long)i * (n1 + 1) + f) * n2 + k) : 0.f;
+    const bool in = e < D::YN && i >= 0 && i < n0 && f >= 0 && f <= n1 && k >= 0 && k < n2;
+    vy[u] = in ? ldT(a.by + ((long long)i * (n1 + 1) + f) * n2 + k) : 0.f;
   }
-  for (int e = tid; e < D::ZN; e += SW_NT) {  // z-faces k0-1 .. k0+TK+1
+#pragma unroll
+  for (int u = 0; u < IZ; ++u) {  // z-faces k0-1 .. k0+TK+1
+    const int e = tid + u * SW_NT;
     const int c = e % (D::CK + 1), t = e / (D::CK + 1), r = t % D::CJ, q = t / D::CJ;
     const int i = i0 - 1 + q, j = j0 - 1 + r, f = k0 - 1 + c;
-    const bool in = i >= 0 && i < n0 && j >= 0 && j < n1 && f >= 0 && f <= n2;
-    sZ[e] = in ? ldT(a.bz + ((long long)i * n1 + j) * (n2 + 1) + f) : 0.f;
+    const bool in = e < D::ZN && i >= 0 && i < n0 && j >= 0 && j < n1 && f >= 0 && f <= n2;
+    vz[u] = in ? ldT(a.bz + ((long long)i * n1 + j) * (n2 + 1) + f) : 0.f;
   }
+#pragma unroll
+  for (int u = 0; u < IP; ++u)
+    if (tid + u * SW_NT < D::PN) sP[tid + u * SW_NT] = vp[u];
+#pragma unroll
+  for (int u = 0; u < IB; ++u)
+    if (tid + u * SW_NT < D::CN) sB[tid + u * SW_NT] = vb[u];
+#pragma unroll
+  for (int u = 0; u < IX; ++u)
+    if (tid + u * SW_NT < D::XN) sX[tid + u * SW_NT] = vx[u];
+#pragma unroll
+  for (int u = 0; u < IY; ++u)
+    if (tid + u * SW_NT < D::YN) sY[tid + u * SW_NT] = vy[u];
+#pragma unroll
+  for (int u = 0; u < IZ; ++u)
+    if (tid + u * SW_NT < D::ZN) sZ[tid + u * SW_NT] = vz[u];
   __syncthreads();
 
   // relax the cell at coefficient-frame coordinates (q, r, c)
@@ -375,6 +415,194 @@ __global__ void __launch_bounds__(SW_NT) k_rb_tile(SweepArgs<T, TB> a) {
       if (tid == 0) {
         a.st->sum_last = v;
         a.st->c_shift = (float)(-(v / (double)a.n_total) * (a.mixed ? (double)a.st->zscale : 1.0));
+        *a.counter = 0u;
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------------- TMA-staged sweep (fp32)
+// Same sweep as k_rb_tile, but one thread stages the five tiles (p with a
+// 2-cell halo; b, x-, y- and z-faces with a 1-cell halo) into shared memory
+// with cp.async.bulk.tensor (TMA, no multicast), completing on an mbarrier.
+// The boxes are 40 floats wide starting at k0 - 4, so every x coordinate is a
+// multiple of 4 floats (16 bytes); cells outside the level read the TMA zero
+// fill.  The mbarrier wait is bounded: on expiry the kernel flags
+// ST_TMA_TIMEOUT, stops the solve and waits (bounded) before returning.
+constexpr int TM_W = 40, TM_X0 = 4;  // box width, k offset of the box start
+
+template <int TI> struct TmaDims {
+  static constexpr int PI = TI + 4, PJ = SW_TJ + 4;
+  static constexpr int CI = TI + 2, CJ = SW_TJ + 2;
+  static constexpr int PN = PI * PJ * TM_W, BN = CI * CJ * TM_W, XN = (CI + 1) * CJ * TM_W, YN = CI * (CJ + 1) * TM_W,
+                       ZN = CI * CJ * TM_W;
+  static constexpr int r128(int b) { return (b + 127) / 128 * 128; }
+  static constexpr int OFF_B = r128(PN * 4), OFF_X = OFF_B + r128(BN * 4), OFF_Y = OFF_X + r128(XN * 4),
+                       OFF_Z = OFF_Y + r128(YN * 4), OFF_BAR = OFF_Z + r128(ZN * 4);
+  static constexpr size_t SMEM = OFF_BAR + 128 + 128;  // + slack to align the base to 128 bytes
+};
+
+struct TileMaps {
+  CUtensorMap p, b, x, y, z;
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+
+constexpr unsigned kTmaWaitLimit = 1u << 22;
+
+template <int TI>
+__global__ void __launch_bounds__(SW_NT) k_rb_tile_tma(const __grid_constant__ TileMaps maps, SweepArgs<float, float> a) {
+  if (is_done(a.st)) return;
+  using D = TmaDims<TI>;
+  extern __shared__ __align__(128) unsigned char tsm_raw[];
+  unsigned char* tsm = tsm_raw + ((128u - (smem_u32(tsm_raw) & 127u)) & 127u);
+  float* sP = reinterpret_cast<float*>(tsm);
+  float* sB = reinterpret_cast<float*>(tsm + D::OFF_B);
+  float* sX = reinterpret_cast<float*>(tsm + D::OFF_X);
+  float* sY = reinterpret_cast<float*>(tsm + D::OFF_Y);
+  float* sZ = reinterpret_cast<float*>(tsm + D::OFF_Z);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tsm + D::OFF_BAR);
+  __shared__ double sred[40];
+  __shared__ int s_fail;
+
+  const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
+  const int k0 = blockIdx.x * SW_TK, j0 = blockIdx.y * SW_TJ, i0 = blockIdx.z * TI;
+  const int tid = threadIdx.x;
+  const long long sI = (long long)n1 * n2;
+  const int hn1 = n1 >> 1, hn2 = n2 >> 1;
+  const bool load_p = !a.zero_in;
+
+  if (tid == 0) {
+    s_fail = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    const unsigned bytes = 4u * (unsigned)((load_p ? D::PN : 0) + D::BN + D::XN + D::YN + D::ZN);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    const int x = k0 - TM_X0;
+    if (load_p) tma_load_3d(sP, &maps.p, x, j0 - 2, i0 - 2, bar);
+    tma_load_3d(sB, &maps.b, x, j0 - 1, i0 - 1, bar);
+    tma_load_3d(sX, &maps.x, x, j0 - 1, i0 - 1, bar);
+    tma_load_3d(sY, &maps.y, x, j0 - 1, i0 - 1, bar);
+    tma_load_3d(sZ, &maps.z, x, j0 - 1, i0 - 1, bar);
+  }
+  if (!load_p)
+    for (int e = tid; e < D::PN; e += SW_NT) sP[e] = 0.f;
+  __syncthreads();  // barrier initialised before anyone waits on it
+  {
+    unsigned it = 0;
+    while (!mbar_try_wait(bar, 0)) {
+      if (++it > kTmaWaitLimit) {
+        s_fail = 1;
+        break;
+      }
+    }
+  }
+  __syncthreads();
+  if (s_fail) {
+    if (tid == 0 && a.st) {
+      a.st->status = ST_TMA_TIMEOUT;
+      a.st->done = 1;
+    }
+    unsigned it = 0;  // give the copies in flight a last bounded chance to land
+    while (!mbar_try_wait(bar, 0) && ++it < kTmaWaitLimit) {
+    }
+    return;
+  }
+  if (a.pc) {  // prolongation folded into the staged p
+    for (int e = tid; e < D::PN; e += SW_NT) {
+      const int c = e % TM_W, t = e / TM_W, r = t % D::PJ, q = t / D::PJ;
+      const int i = i0 - 2 + q, j = j0 - 2 + r, k = k0 - TM_X0 + c;
+      if (i >= 0 && i < n0 && j >= 0 && j < n1 && k >= 0 && k < n2)
+        sP[e] += a.pc[((long long)(i >> 1) * hn1 + (j >> 1)) * hn2 + (k >> 1)] * a.pc_scale;
+    }
+    __syncthreads();
+  }
+
+  // relax the cell at coefficient-frame coordinates (q, r, c), c = k - (k0 - 1)
+  auto relax = [&](int q, int r, int c) {
+    float* pp = sP + ((q + 1) * D::PJ + (r + 1)) * TM_W + (c + TM_X0 - 1);
+    const int ce = (q * D::CJ + r) * TM_W + (c + TM_X0 - 1);
+    const float bxl = sX[ce], bxu = sX[ce + D::CJ * TM_W];
+    const int ye = (q * (D::CJ + 1) + r) * TM_W + (c + TM_X0 - 1);
+    const float byl = sY[ye], byu = sY[ye + TM_W];
+    const float bzl = sZ[ce], bzu = sZ[ce + 1];
+    bool ok;
+    const float v = gs_update(*pp, pp[-D::PJ * TM_W], pp[D::PJ * TM_W], pp[-TM_W], pp[TM_W], pp[-1], pp[1], bxl, bxu,
+                              byl, byu, bzl, bzu, sB[ce], a.omega, a.flux, &ok);
+    if (ok) *pp = v;
+  };
+  const int c1 = a.first_color, c2 = c1 ^ 1;
+  {
+    constexpr int HALF = (SW_TK + 2) / 2;  // 17 cells of one colour per ring row
+    for (int e = tid; e < D::CI * D::CJ * HALF; e += SW_NT) {
+      const int h = e % HALF, row = e / HALF, r = row % D::CJ, q = row / D::CJ;
+      const int i = i0 - 1 + q, j = j0 - 1 + r;
+      const int par = (c1 - i - j - (k0 - 1)) & 1;
+      const int c = 2 * h + par, k = k0 - 1 + c;
+      if (i < 0 || i >= n0 || j < 0 || j >= n1 || k < 0 || k >= n2) continue;
+      relax(q, r, c);
+    }
+  }
+  __syncthreads();
+  {
+    constexpr int HALF = SW_TK / 2;
+    for (int e = tid; e < TI * SW_TJ * HALF; e += SW_NT) {
+      const int h = e % HALF, row = e / HALF, r = row % SW_TJ, q = row / SW_TJ;
+      const int i = i0 + q, j = j0 + r;
+      const int par = (c2 - i - j - k0) & 1;
+      const int c = 2 * h + par, k = k0 + c;
+      if (i >= n0 || j >= n1 || k >= n2) continue;
+      relax(q + 1, r + 1, c + 1);
+    }
+  }
+  __syncthreads();
+  double msum = 0.0;
+  for (int e = tid; e < TI * SW_TJ * SW_TK; e += SW_NT) {
+    const int c = e % SW_TK, t = e / SW_TK, r = t % SW_TJ, q = t / SW_TJ;
+    const int i = i0 + q, j = j0 + r, k = k0 + c;
+    if (i >= n0 || j >= n1 || k >= n2) continue;
+    const float v = sP[((q + 2) * D::PJ + (r + 2)) * TM_W + (c + TM_X0)];
+    a.p_out[i * sI + (long long)j * n2 + k] = v;
+    if (a.partials) msum += (double)v;
+  }
+  if (a.partials) {
+    const double bs = block_sum<SW_NT>(msum, sred);
+    const int nb = gridDim.x * gridDim.y * gridDim.z;
+    const int bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    __shared__ bool s_last;
+    if (tid == 0) {
+      a.partials[bid] = bs;
+      __threadfence();
+      s_last = (atomicAdd(a.counter, 1u) == (unsigned)nb - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      double v = 0.0;
+      for (int q = tid; q < nb; q += SW_NT) v += ((volatile double*)a.partials)[q];
+      v = block_sum<SW_NT>(v, sred);
+      if (tid == 0) {
+        a.st->sum_last = v;
+        a.st->c_shift = (float)(-(v / (double)a.n_total));
         *a.counter = 0u;
       }
     }
@@ -456,6 +684,7 @@ constexpr int BT_NT = 1024;
 
 struct BottomLevel {
   int n0, n1, n2;
+  int s1, s2;  // log2(n1), log2(n2) when both are powers of two, else -1
   const void* bx;
   const void* by;
   const void* bz;
@@ -478,6 +707,21 @@ template <class T, class TB> struct BottomArgs {
 __host__ __device__ inline size_t bottom_level_floats(int n0, int n1, int n2) {
   const size_t n = (size_t)n0 * n1 * n2;
   return 2 * n + (size_t)(n0 + 1) * n1 * n2 + (size_t)n0 * (n1 + 1) * n2 + (size_t)n0 * n1 * (n2 + 1);
+}
+
+// cell (i,j,k) of linear index e
+__device__ __forceinline__ void bt_ijk(const BottomLevel& L, int e, int& i, int& j, int& k) {
+  if (L.s1 >= 0) {
+    k = e & (L.n2 - 1);
+    const int t = e >> L.s2;
+    j = t & (L.n1 - 1);
+    i = t >> L.s1;
+  } else {
+    k = e % L.n2;
+    const int t = e / L.n2;
+    j = t % L.n1;
+    i = t / L.n1;
+  }
 }
 
 // in-place relax of cell (i,j,k) of a shared-memory level, clamped neighbours
@@ -514,6 +758,48 @@ __device__ __forceinline__ void bt_relax(R* P, const float* B, const float* X, c
   P[e] = pv + omega * res / d;
 }
 
+// one half-sweep (cells of `color`) over a level with nt threads starting at tid
+template <class R>
+__device__ __forceinline__ void bt_half_sweep(const BottomLevel& L, R* P, const float* B, const float* X,
+                                              const float* Y, const float* Z, int color, R omega, int flux, int tid,
+                                              int nt) {
+  const int n0 = L.n0, n1 = L.n1, n2 = L.n2;
+  if ((n2 & 1) == 0) {  // only the cells of this colour: two per pair along k
+    const int hn = (n0 * n1 * n2) >> 1, hk = n2 >> 1;
+    for (int e = tid; e < hn; e += nt) {
+      const int h = e % hk, row = e / hk, j = row % n1, i = row / n1;
+      const int k = 2 * h + ((color - i - j) & 1);
+      bt_relax<R>(P, B, X, Y, Z, n0, n1, n2, i, j, k, omega, flux);
+    }
+  } else {
+    const int n = n0 * n1 * n2;
+    for (int e = tid; e < n; e += nt) {
+      int i, j, k;
+      bt_ijk(L, e, i, j, k);
+      if (((i + j + k) & 1) != color) continue;
+      bt_relax<R>(P, B, X, Y, Z, n0, n1, n2, i, j, k, omega, flux);
+    }
+  }
+}
+
+// dst[e] = src[e] (converted) for e < n, loads issued 8 at a time
+template <class T>
+__device__ __forceinline__ void bt_load(float* dst, const T* src, int n, float scale, int tid) {
+  for (int base = tid; base < n; base += 8 * BT_NT) {
+    float v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = base + u * BT_NT;
+      v[u] = (e < n) ? ldT(src + e) * scale : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = base + u * BT_NT;
+      if (e < n) dst[e] = v[u];
+    }
+  }
+}
+
 template <class T, class TB, class AccT>
 __global__ void __launch_bounds__(BT_NT) k_bottom(BottomArgs<T, TB> a) {
   if (is_done(a.st)) return;
@@ -521,88 +807,78 @@ __global__ void __launch_bounds__(BT_NT) k_bottom(BottomArgs<T, TB> a) {
   __shared__ double sred[40];
   __shared__ double s_mean;
   const int tid = threadIdx.x;
-  // carve the levels
-  float* Pl[PF_MG_MAX_LEVELS];
-  float* Bl[PF_MG_MAX_LEVELS];
-  float* Xl[PF_MG_MAX_LEVELS];
-  float* Yl[PF_MG_MAX_LEVELS];
-  float* Zl[PF_MG_MAX_LEVELS];
-  {
-    float* cur = reinterpret_cast<float*>(btsm);
-    for (int l = 0; l < a.nl; ++l) {
-      const int n0 = a.L[l].n0, n1 = a.L[l].n1, n2 = a.L[l].n2, n = n0 * n1 * n2;
-      Pl[l] = cur; cur += n;
-      Bl[l] = cur; cur += n;
-      Xl[l] = cur; cur += (n0 + 1) * n1 * n2;
-      Yl[l] = cur; cur += n0 * (n1 + 1) * n2;
-      Zl[l] = cur; cur += n0 * n1 * (n2 + 1);
-    }
-  }
-  AccT* Pc;  // coarsest level in AccT, after the float levels
-  {
-    const BottomLevel& Lc = a.L[a.nl - 1];
-    float* end = Zl[a.nl - 1] + Lc.n0 * Lc.n1 * (Lc.n2 + 1);
-    uintptr_t u = (reinterpret_cast<uintptr_t>(end) + 15) & ~uintptr_t(15);
-    Pc = reinterpret_cast<AccT*>(u);
-  }
-  // load faces of every level and b of the top level; zero p
-  const float bsc = a.b_scale ? *a.b_scale : 1.f;
-  for (int l = 0; l < a.nl; ++l) {
+  const int nl = a.nl;
+  // level l starts at float offset base(l); arrays P, B, X, Y, Z in that order
+  auto base = [&](int l) {
+    size_t off = 0;
+    for (int q = 0; q < l; ++q) off += bottom_level_floats(a.L[q].n0, a.L[q].n1, a.L[q].n2);
+    return reinterpret_cast<float*>(btsm) + off;
+  };
+  struct LvPtr {
+    float *P, *B, *X, *Y, *Z;
+  };
+  auto ptrs = [&](int l) {
     const int n0 = a.L[l].n0, n1 = a.L[l].n1, n2 = a.L[l].n2, n = n0 * n1 * n2;
-    const int nfx = (n0 + 1) * n1 * n2, nfy = n0 * (n1 + 1) * n2, nfz = n0 * n1 * (n2 + 1);
-    const T* gx = reinterpret_cast<const T*>(a.L[l].bx);
-    const T* gy = reinterpret_cast<const T*>(a.L[l].by);
-    const T* gz = reinterpret_cast<const T*>(a.L[l].bz);
-    for (int e = tid; e < nfx; e += BT_NT) Xl[l][e] = ldT(gx + e);
-    for (int e = tid; e < nfy; e += BT_NT) Yl[l][e] = ldT(gy + e);
-    for (int e = tid; e < nfz; e += BT_NT) Zl[l][e] = ldT(gz + e);
-    for (int e = tid; e < n; e += BT_NT) Pl[l][e] = 0.f;
+    LvPtr r;
+    r.P = base(l);
+    r.B = r.P + n;
+    r.X = r.B + n;
+    r.Y = r.X + (n0 + 1) * n1 * n2;
+    r.Z = r.Y + n0 * (n1 + 1) * n2;
+    return r;
+  };
+  AccT* Pc;
+  {
+    float* end = base(nl);
+    Pc = reinterpret_cast<AccT*>((reinterpret_cast<uintptr_t>(end) + 15) & ~uintptr_t(15));
+  }
+  // ---- load faces of every level and b of the top level; zero p
+  for (int l = 0; l < nl; ++l) {
+    const BottomLevel& L = a.L[l];
+    const LvPtr q = ptrs(l);
+    const int n = L.n0 * L.n1 * L.n2;
+    bt_load(q.X, reinterpret_cast<const T*>(L.bx), (L.n0 + 1) * L.n1 * L.n2, 1.f, tid);
+    bt_load(q.Y, reinterpret_cast<const T*>(L.by), L.n0 * (L.n1 + 1) * L.n2, 1.f, tid);
+    bt_load(q.Z, reinterpret_cast<const T*>(L.bz), L.n0 * L.n1 * (L.n2 + 1), 1.f, tid);
+    for (int e = tid; e < n; e += BT_NT) q.P[e] = 0.f;
   }
   {
-    const int n = a.L[0].n0 * a.L[0].n1 * a.L[0].n2;
-    for (int e = tid; e < n; e += BT_NT) Bl[0][e] = ldT(a.b + e) * bsc;
+    const LvPtr q = ptrs(0);
+    bt_load(q.B, a.b, a.L[0].n0 * a.L[0].n1 * a.L[0].n2, a.b_scale ? *a.b_scale : 1.f, tid);
   }
   __syncthreads();
   const float om = a.omega;
-  auto smooth = [&](int l, int nsweeps, int first) {
-    const int n0 = a.L[l].n0, n1 = a.L[l].n1, n2 = a.L[l].n2, n = n0 * n1 * n2;
-    for (int s = 0; s < nsweeps; ++s) {
+  // ---- down: pre-smoothing, residual, restriction
+  for (int l = 0; l < nl - 1; ++l) {
+    const BottomLevel& L = a.L[l];
+    const LvPtr q = ptrs(l);
+    for (int sw = 0; sw < a.pre; ++sw)
       for (int cc = 0; cc < 2; ++cc) {
-        const int color = first ^ cc;
-        for (int e = tid; e < n; e += BT_NT) {
-          const int k = e % n2, t = e / n2, j = t % n1, i = t / n1;
-          if (((i + j + k) & 1) != color) continue;
-          bt_relax<float>(Pl[l], Bl[l], Xl[l], Yl[l], Zl[l], n0, n1, n2, i, j, k, om, a.flux);
-        }
+        bt_half_sweep<float>(L, q.P, q.B, q.X, q.Y, q.Z, cc, om, a.flux, tid, BT_NT);
         __syncthreads();
       }
-    }
-  };
-  // ---- down
-  for (int l = 0; l < a.nl - 1; ++l) {
-    smooth(l, a.pre, 0);
-    const int n0 = a.L[l].n0, n1 = a.L[l].n1, n2 = a.L[l].n2;
-    const int C0 = n0 >> 1, C1 = n1 >> 1, C2 = n2 >> 1, nc = C0 * C1 * C2;
-    const float* P = Pl[l];
-    const float* B = Bl[l];
-    const float* X = Xl[l];
-    const float* Y = Yl[l];
-    const float* Z = Zl[l];
+    const int n0 = L.n0, n1 = L.n1, n2 = L.n2;
+    const int C1 = n1 >> 1, C2 = n2 >> 1, nc = (n0 >> 1) * C1 * C2;
+    float* Bc = ptrs(l + 1).B;
     const int sI = n1 * n2;
     for (int ec = tid; ec < nc; ec += BT_NT) {
       const int K = ec % C2, t = ec / C2, J = t % C1, I = t / C1;
       float acc = 0.f;
+#pragma unroll
       for (int aa = 0; aa < 2; ++aa)
+#pragma unroll
         for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
           for (int cc = 0; cc < 2; ++cc) {
             const int i = 2 * I + aa, j = 2 * J + bb, k = 2 * K + cc;
             const int e = (i * n1 + j) * n2 + k;
             const int fyi = (i * (n1 + 1) + j) * n2 + k, fzi = (i * n1 + j) * (n2 + 1) + k;
-            const float bxl = X[e], bxu = X[e + sI], byl = Y[fyi], byu = Y[fyi + n2], bzl = Z[fzi], bzu = Z[fzi + 1];
-            const float pv = P[e];
-            const float q0 = P[i > 0 ? e - sI : e], q1 = P[i < n0 - 1 ? e + sI : e];
-            const float q2 = P[j > 0 ? e - n2 : e], q3 = P[j < n1 - 1 ? e + n2 : e];
-            const float q4 = P[k > 0 ? e - 1 : e], q5 = P[k < n2 - 1 ? e + 1 : e];
+            const float bxl = q.X[e], bxu = q.X[e + sI], byl = q.Y[fyi], byu = q.Y[fyi + n2], bzl = q.Z[fzi],
+                        bzu = q.Z[fzi + 1];
+            const float pv = q.P[e];
+            const float q0 = q.P[i > 0 ? e - sI : e], q1 = q.P[i < n0 - 1 ? e + sI : e];
+            const float q2 = q.P[j > 0 ? e - n2 : e], q3 = q.P[j < n1 - 1 ? e + n2 : e];
+            const float q4 = q.P[k > 0 ? e - 1 : e], q5 = q.P[k < n2 - 1 ? e + 1 : e];
             float Ap;
             if (a.flux) {
               float sm = bxl * (pv - q0);
@@ -622,29 +898,26 @@ __global__ void __launch_bounds__(BT_NT) k_bottom(BottomArgs<T, TB> a) {
               sm += bzu * q5;
               Ap = d * pv - sm;
             }
-            acc += B[e] - Ap;
+            acc += q.B[e] - Ap;
           }
-      Bl[l + 1][ec] = roundT<T>(acc * a.rscale);
+      Bc[ec] = roundT<T>(acc * a.rscale);
     }
     __syncthreads();
   }
-  // ---- coarsest
+  // ---- coarsest: sweeps from zero in AccT, then mean removal
   {
-    const int l = a.nl - 1;
-    const int n0 = a.L[l].n0, n1 = a.L[l].n1, n2 = a.L[l].n2, n = n0 * n1 * n2;
+    const BottomLevel& L = a.L[nl - 1];
+    const LvPtr q = ptrs(nl - 1);
+    const int n = L.n0 * L.n1 * L.n2;
     for (int e = tid; e < n; e += BT_NT) Pc[e] = AccT(0);
     __syncthreads();
     const bool one_warp = n <= 256;
     const AccT omc = (AccT)om;
     if (!one_warp || tid < 32) {
       const int nt = one_warp ? 32 : BT_NT;
-      for (int s = 0; s < a.coarsest; ++s) {
+      for (int sw = 0; sw < a.coarsest; ++sw) {
         for (int color = 0; color < 2; ++color) {
-          for (int e = tid; e < n; e += nt) {
-            const int k = e % n2, t = e / n2, j = t % n1, i = t / n1;
-            if (((i + j + k) & 1) != color) continue;
-            bt_relax<AccT>(Pc, Bl[l], Xl[l], Yl[l], Zl[l], n0, n1, n2, i, j, k, omc, a.flux);
-          }
+          bt_half_sweep<AccT>(L, Pc, q.B, q.X, q.Y, q.Z, color, omc, a.flux, tid, nt);
           if (one_warp) __syncwarp();
           else __syncthreads();
         }
@@ -657,26 +930,34 @@ __global__ void __launch_bounds__(BT_NT) k_bottom(BottomArgs<T, TB> a) {
     if (tid == 0) s_mean = tot / (double)n;
     __syncthreads();
     const AccT shift = (AccT)(-s_mean);
-    for (int e = tid; e < n; e += BT_NT) Pl[l][e] = roundT<T>((float)(Pc[e] + shift));
+    for (int e = tid; e < n; e += BT_NT) q.P[e] = roundT<T>((float)(Pc[e] + shift));
     __syncthreads();
   }
-  // ---- up
-  for (int l = a.nl - 2; l >= 0; --l) {
-    const int n0 = a.L[l].n0, n1 = a.L[l].n1, n2 = a.L[l].n2, n = n0 * n1 * n2;
-    const int h1 = n1 >> 1, h2 = n2 >> 1;
+  // ---- up: prolongation, post-smoothing with the colours reversed
+  for (int l = nl - 2; l >= 0; --l) {
+    const BottomLevel& L = a.L[l];
+    const LvPtr q = ptrs(l);
+    const float* Pcoarse = ptrs(l + 1).P;
+    const int n = L.n0 * L.n1 * L.n2, h1 = L.n1 >> 1, h2 = L.n2 >> 1;
     for (int e = tid; e < n; e += BT_NT) {
-      const int k = e % n2, t = e / n2, j = t % n1, i = t / n1;
-      Pl[l][e] += Pl[l + 1][((i >> 1) * h1 + (j >> 1)) * h2 + (k >> 1)] * a.pscale;
+      int i, j, k;
+      bt_ijk(L, e, i, j, k);
+      q.P[e] += Pcoarse[((i >> 1) * h1 + (j >> 1)) * h2 + (k >> 1)] * a.pscale;
     }
     __syncthreads();
-    smooth(l, a.post, 1);
+    for (int sw = 0; sw < a.post; ++sw)
+      for (int cc = 0; cc < 2; ++cc) {
+        bt_half_sweep<float>(L, q.P, q.B, q.X, q.Y, q.Z, 1 ^ cc, om, a.flux, tid, BT_NT);
+        __syncthreads();
+      }
   }
   // ---- output (and the mean when the top level is level 0)
+  const float* P0 = ptrs(0).P;
   const int n = a.L[0].n0 * a.L[0].n1 * a.L[0].n2;
   double ls = 0.0;
   for (int e = tid; e < n; e += BT_NT) {
-    stT(a.p_out + e, Pl[0][e]);
-    ls += (double)roundT<T>(Pl[0][e]);
+    stT(a.p_out + e, P0[e]);
+    ls += (double)roundT<T>(P0[e]);
   }
   if (a.want_mean) {
     const double tot = block_sum<BT_NT>(ls, sred);
@@ -980,6 +1261,7 @@ struct pf_mg_plan {
   int prec;
   float lp_scale[PF_MG_MAX_LEVELS];
   int lb;              // first level solved by the single-CTA bottom kernel (nlev = none)
+  bool use_tma;        // stage fp32 smoother tiles with TMA where the level allows it
   size_t bottom_smem;  // dynamic shared memory of the bottom kernel
   cudaStream_t cap_stream;
   cudaGraphExec_t exec[2];
@@ -1008,8 +1290,63 @@ template <class T> LV<T> view(pf_mg_plan* P, int lv) {
   return LV<T>{(T*)L.bx_lp, (T*)L.by_lp, (T*)L.bz_lp, (T*)L.p_lp, (T*)L.p_lp_alt, (T*)L.b_lp};
 }
 
-int red_grid(long long n) { return grid_for(n, RED_NT, RED_MAX_BLOCKS); }
-int ew_grid(long long n) { return grid_for(n, 256, kNumSMs * 16); }
+// one thread per element: every load of a thread is independent of the others
+int red_grid(long long n) { return grid_for(n, RED_NT, (int)(pf::kPartials / 2)); }
+int ew_grid(long long n) { return grid_for(n, 256, 1 << 20); }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(ptr);
+    cudaGetLastError();
+  }
+  return fn;
+}
+
+// 3D fp32 tensor: extents (d0 innermost, d1, d2), row pitch and plane pitch in floats
+bool encode3d(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint64_t d2, uint64_t row_pitch,
+              uint64_t plane_pitch, uint32_t b0, uint32_t b1, uint32_t b2) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn || !aligned16(base) || (row_pitch * 4) % 16 || (plane_pitch * 4) % 16) return false;
+  cuuint64_t dims[3] = {d0, d1, d2};
+  cuuint64_t strides[2] = {row_pitch * 4, plane_pitch * 4};
+  cuuint32_t box[3] = {b0, b1, b2};
+  cuuint32_t es[3] = {1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// TMA staging of a level: fp32 storage, rows a multiple of 4 floats, padded z-faces
+template <class T, class TB>
+bool tma_maps(pf_mg_plan* P, int lv, const T* p_in, const TB* b, const float* b_scale, const LV<T>& V, TileMaps* m) {
+  if constexpr (!std::is_same<T, float>::value || !std::is_same<TB, float>::value) {
+    return false;
+  } else {
+    const pf_mg_level& L = P->d.lev[lv];
+    if (b_scale || !L.bz_pad || L.nz % 4 != 0 || L.bz_pitch % 8 != 0) return false;
+    constexpr int TI = 4;
+    const uint64_t n0 = L.nx, n1 = L.ny, n2 = L.nz;
+    const float* pm = p_in ? p_in : V.p0;
+    return encode3d(&m->p, pm, n2, n1, n0, n2, n1 * n2, TM_W, SW_TJ + 4, TI + 4) &&
+           encode3d(&m->b, b, n2, n1, n0, n2, n1 * n2, TM_W, SW_TJ + 2, TI + 2) &&
+           encode3d(&m->x, V.bx, n2, n1, n0 + 1, n2, n1 * n2, TM_W, SW_TJ + 2, TI + 3) &&
+           encode3d(&m->y, V.by, n2, n1 + 1, n0, n2, (n1 + 1) * n2, TM_W, SW_TJ + 3, TI + 2) &&
+           encode3d(&m->z, L.bz_pad, n2 + 1, n1, n0, (uint64_t)L.bz_pitch, n1 * (uint64_t)L.bz_pitch, TM_W,
+                    SW_TJ + 2, TI + 2);
+  }
+}
 
 template <class T, class TB>
 int launch_sweep(pf_mg_plan* P, int lv, const T* p_in, bool zero_in, T* p_out, const TB* b, const float* b_scale,
@@ -1032,6 +1369,14 @@ int launch_sweep(pf_mg_plan* P, int lv, const T* p_in, bool zero_in, T* p_out, c
   a.flux = P->d.stencil == PF_STENCIL_FLUX ? 1 : 0;
   constexpr int TI = 4;
   dim3 grid((L.nz + SW_TK - 1) / SW_TK, (L.ny + SW_TJ - 1) / SW_TJ, (L.nx + TI - 1) / TI);
+  if constexpr (std::is_same<T, float>::value && std::is_same<TB, float>::value) {
+    TileMaps maps;
+    if (P->use_tma && tma_maps<T, TB>(P, lv, p_in, b, b_scale, V, &maps)) {
+      k_rb_tile_tma<TI><<<grid, SW_NT, TmaDims<TI>::SMEM, s>>>(maps, a);
+      PF_LAUNCHED();
+      return PF_OK;
+    }
+  }
   k_rb_tile<T, TB, TI><<<grid, SW_NT, TileDims<TI>::SMEM, s>>>(a);
   PF_LAUNCHED();
   return PF_OK;
@@ -1045,7 +1390,14 @@ int launch_bottom(pf_mg_plan* P, const TB* b, const float* b_scale, bool want_me
   for (int l = 0; l < a.nl; ++l) {
     const pf_mg_level& L = P->d.lev[lb + l];
     LV<T> V = view<T>(P, lb + l);
-    a.L[l] = BottomLevel{L.nx, L.ny, L.nz, V.bx, V.by, V.bz};
+    auto lg = [](int v) {
+      int s = 0;
+      while ((1 << s) < v) ++s;
+      return (1 << s) == v ? s : -1;
+    };
+    const int s1 = lg(L.ny), s2 = lg(L.nz);
+    const bool p2 = s1 >= 0 && s2 >= 0;
+    a.L[l] = BottomLevel{L.nx, L.ny, L.nz, p2 ? s1 : -1, p2 ? s2 : -1, V.bx, V.by, V.bz};
   }
   LV<T> V0 = view<T>(P, lb);
   a.b = b;
@@ -1289,7 +1641,8 @@ template <class T> int build_impl(pf_mg_plan* P, cudaStream_t s) {
                          (long long)L.nx * L.ny * (L.nz + 1);
     T* lpx = mixed(P) ? (T*)L.bx_lp : nullptr;
     k_level_coefs<T><<<ew_grid(n + (lpx ? nf : 0)), 256, 0, s>>>(L.nx, L.ny, L.nz, L.bx, L.by, L.bz, L.diag, lpx,
-                                                                 (T*)L.by_lp, (T*)L.bz_lp, P->lp_scale[lv]);
+                                                                 (T*)L.by_lp, (T*)L.bz_lp, P->lp_scale[lv],
+                                                                 L.bz_pad, L.bz_pitch);
     PF_LAUNCHED();
     if (lv + 1 < P->d.nlev) {
       const pf_mg_level& C = P->d.lev[lv + 1];
@@ -1330,6 +1683,7 @@ template <class T> cudaError_t set_smem_attrs() {
   chk(cudaFuncSetAttribute(k_bottom<T, T, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   chk(cudaFuncSetAttribute(k_rb_tile<T, float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile));
   chk(cudaFuncSetAttribute(k_rb_tile<T, T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile));
+  chk(cudaFuncSetAttribute(k_rb_tile_tma<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TmaDims<4>::SMEM));
   return e;
 }
 
@@ -1377,6 +1731,10 @@ int pf_mg_plan_create(const pf_mg_desc* desc, pf_mg_plan** out) {
   std::memset(P, 0, sizeof(*P));
   P->d = *desc;
   P->prec = desc->precision;
+  {
+    const char* env = std::getenv("PFFLIP_NO_TMA");
+    P->use_tma = !(env && env[0] == '1');
+  }
   for (int lv = 0; lv < desc->nlev; ++lv) {
     const pf_mg_level& L = desc->lev[lv];
     P->lp_scale[lv] = std::ldexp(desc->coef_scale > 0.f ? desc->coef_scale : 1.f, -2 * lv);

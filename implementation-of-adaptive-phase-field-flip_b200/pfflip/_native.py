@@ -50,6 +50,7 @@ class pf_mg_level(C.Structure):
         ("p", C.c_void_p), ("p_alt", C.c_void_p), ("b", C.c_void_p), ("r", C.c_void_p),
         ("bx_lp", C.c_void_p), ("by_lp", C.c_void_p), ("bz_lp", C.c_void_p),
         ("p_lp", C.c_void_p), ("p_lp_alt", C.c_void_p), ("b_lp", C.c_void_p),
+        ("bz_pad", C.c_void_p), ("bz_pitch", C.c_int32),
     ]
 
 

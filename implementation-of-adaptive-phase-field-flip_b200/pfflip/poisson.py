@@ -49,6 +49,9 @@ class _Level:
         self.b = z((nx, ny, nz))
         self.r = z((nx, ny, nz))
         self.p_alt = z((nx, ny, nz))
+        # z-faces with rows padded to a multiple of 8 floats for TMA staging
+        self.bz_pitch = (nz + 1 + 7) // 8 * 8
+        self.bz_pad = z((nx, ny, self.bz_pitch)) if nz % 4 == 0 else None
         self.lp = None
         if precision in _LP_DTYPE:
             dt = _LP_DTYPE[precision]
@@ -63,6 +66,8 @@ class _Level:
         d.nx, d.ny, d.nz = self.res
         d.bx, d.by, d.bz, d.diag = (N.ptr(a) for a in (self.bx, self.by, self.bz, self.diag))
         d.p, d.p_alt, d.b, d.r = (N.ptr(a) for a in (self.p, self.p_alt, self.b, self.r))
+        if self.bz_pad is not None:
+            d.bz_pad, d.bz_pitch = N.ptr(self.bz_pad), self.bz_pitch
         if self.lp:
             lp = self.lp
             d.bx_lp, d.by_lp, d.bz_lp = N.ptr(lp["bx"]), N.ptr(lp["by"]), N.ptr(lp["bz"])

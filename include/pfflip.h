@@ -192,6 +192,12 @@ typedef struct pf_mg_level {
   float *b, *r;               /* right-hand side, residual */
   void *bx_lp, *by_lp, *bz_lp;
   void *p_lp, *p_lp_alt, *b_lp;
+  /* optional copy of bz with rows padded to bz_pitch floats (bz_pitch a multiple
+   * of 8, >= nz+1), filled by pf_mg_build_hierarchy: lets the fp32 smoother
+   * stage z-faces with TMA, whose row pitch must be a multiple of 16 bytes.
+   * NULL: that level's smoother stages through registers. */
+  float* bz_pad;
+  int32_t bz_pitch;
 } pf_mg_level;
 
 /* Multigrid-preconditioned flexible CG; mirrors pfflip/poisson.py:240-274
