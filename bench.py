@@ -65,6 +65,11 @@ def parse():
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--solve-oracle", action="store_true", help="also solve the 128^3 problem with the FP64 oracle")
+    ap.add_argument("--solve-only", action="store_true", help="only the standalone solve leg (prints its JSON)")
+    ap.add_argument("--solve-variants", default="fp32_flux,fp16_flux,bf16_flux,fp32_reference",
+                    help="comma list of precision_stencil variants for the solve leg")
+    ap.add_argument("--solve-repeats", type=int, default=5)
+    ap.add_argument("--no-graphs", action="store_true", help="solve leg without CUDA graphs")
     return ap.parse_args()
 
 
@@ -380,14 +385,15 @@ def solve_leg(args):
         from oracle import oracle as O
 
         ref64, _, _ = O.fp64_reference_solve(bx, by, bz, b.astype(np.float64), tol=1e-12)
-    for prec, stencil in (("fp32", "flux"), ("fp16", "flux"), ("bf16", "flux"), ("fp32", "reference")):
-        s = MGPCG((r, r, r), "cuda", pre=3, post=3, precision=prec, stencil=stencil)
+    for var in args.solve_variants.split(","):
+        prec, stencil = var.split("_")
+        s = MGPCG((r, r, r), "cuda", pre=3, post=3, precision=prec, stencil=stencil, use_graphs=not args.no_graphs)
         s.build_hierarchy(dev(bx), dev(by), dev(bz))
         x = DeviceArray.zeros((r, r, r))
         bd = dev(b)
         s.solve(bd, x, tol=1e-6, max_iter=100)  # warm-up (graph capture)
         ts = []
-        for _ in range(5):
+        for _ in range(args.solve_repeats):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()
             e0.record()
@@ -435,6 +441,12 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.solve_only:
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps({"solve": solve_leg(args)}), flush=True)
+        return 0
     return run_ours(args)
 
 

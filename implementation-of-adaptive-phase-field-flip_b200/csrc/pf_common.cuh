@@ -133,25 +133,32 @@ template <int NT> __device__ __forceinline__ float block_max(float v, float* sh 
   return r;
 }
 
-// Deterministic grid reduction: every block writes its partial, the last
-// block to arrive (ticket on *counter) sums the partials in block order with a
-// fixed tree and resets the counter.  Returns true in the last block (all
-// threads), with *result valid in every thread of that block.
+// Deterministic grid reduction over a grid of any shape: every block writes
+// its partial at its linear block id, the last block to arrive (ticket on
+// *counter) sums the partials in block order with a fixed tree and resets the
+// counter.  Returns true in the last block (all threads), with *result valid
+// in every thread of that block.  The partials are read from L2 (__ldcg):
+// they were written by other blocks before their fenced ticket.
+__device__ __forceinline__ unsigned lin_block() { return (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x; }
+__device__ __forceinline__ unsigned num_blocks() { return gridDim.x * gridDim.y * gridDim.z; }
+
 template <int NT>
 __device__ __forceinline__ bool grid_sum_last(double partial_in_t0, double* partials, unsigned* counter,
                                               double* result, double* sh) {
   __shared__ bool s_last;
+  const unsigned nb = num_blocks();
   if (threadIdx.x == 0) {
-    partials[blockIdx.x] = partial_in_t0;
+    partials[lin_block()] = partial_in_t0;
     __threadfence();
     unsigned t = atomicAdd(counter, 1u);
-    s_last = (t == gridDim.x - 1);
+    s_last = (t == nb - 1);
   }
   __syncthreads();
   if (!s_last) return false;
   __threadfence();
   double v = 0.0;
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += NT) v += ((volatile double*)partials)[b];
+#pragma unroll 8
+  for (unsigned b = threadIdx.x; b < nb; b += NT) v += __ldcg(partials + b);
   v = block_sum<NT>(v, sh);
   if (threadIdx.x == 0) {
     sh[32] = v;
@@ -162,25 +169,28 @@ __device__ __forceinline__ bool grid_sum_last(double partial_in_t0, double* part
   return true;
 }
 
-// Two sums at once (same protocol; partials holds 2*gridDim.x doubles).
+// Two sums at once (same protocol; partials holds 2 * blocks doubles).
 template <int NT>
 __device__ __forceinline__ bool grid_sum2_last(double a_t0, double b_t0, double* partials, unsigned* counter,
                                                double* ra, double* rb, double* sh) {
   __shared__ bool s_last;
+  const unsigned nb = num_blocks();
   if (threadIdx.x == 0) {
-    partials[2 * blockIdx.x] = a_t0;
-    partials[2 * blockIdx.x + 1] = b_t0;
+    const unsigned id = lin_block();
+    partials[2 * id] = a_t0;
+    partials[2 * id + 1] = b_t0;
     __threadfence();
     unsigned t = atomicAdd(counter, 1u);
-    s_last = (t == gridDim.x - 1);
+    s_last = (t == nb - 1);
   }
   __syncthreads();
   if (!s_last) return false;
   __threadfence();
   double va = 0.0, vb = 0.0;
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += NT) {
-    va += ((volatile double*)partials)[2 * b];
-    vb += ((volatile double*)partials)[2 * b + 1];
+#pragma unroll 8
+  for (unsigned b = threadIdx.x; b < nb; b += NT) {
+    va += __ldcg(partials + 2 * b);
+    vb += __ldcg(partials + 2 * b + 1);
   }
   va = block_sum<NT>(va, sh);
   vb = block_sum<NT>(vb, sh);
@@ -199,17 +209,19 @@ template <int NT>
 __device__ __forceinline__ bool grid_max_last(float partial_in_t0, double* partials, unsigned* counter,
                                               float* result, float* shf) {
   __shared__ bool s_last;
+  const unsigned nb = num_blocks();
   if (threadIdx.x == 0) {
-    partials[blockIdx.x] = (double)partial_in_t0;
+    partials[lin_block()] = (double)partial_in_t0;
     __threadfence();
     unsigned t = atomicAdd(counter, 1u);
-    s_last = (t == gridDim.x - 1);
+    s_last = (t == nb - 1);
   }
   __syncthreads();
   if (!s_last) return false;
   __threadfence();
   float v = 0.f;
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += NT) v = fmaxf(v, (float)((volatile double*)partials)[b]);
+#pragma unroll 8
+  for (unsigned b = threadIdx.x; b < nb; b += NT) v = fmaxf(v, (float)__ldcg(partials + b));
   v = block_max<NT>(v, shf);
   if (threadIdx.x == 0) {
     shf[32] = v;
@@ -218,6 +230,20 @@ __device__ __forceinline__ bool grid_max_last(float partial_in_t0, double* parti
   __syncthreads();
   *result = shf[32];
   return true;
+}
+
+// 3D launch shape for cell-wise kernels: 256 threads = 8 rows (j) of 32 cells
+// (k), blockIdx.z = i.  Index math is shifts and adds only.
+constexpr int C3_TK = 32, C3_TJ = 8, C3_NT = 256;
+inline dim3 grid_cells(int n0, int n1, int n2) {
+  return dim3((unsigned)((n2 + C3_TK - 1) / C3_TK), (unsigned)((n1 + C3_TJ - 1) / C3_TJ), (unsigned)n0);
+}
+struct Cell3 {
+  int i, j, k;
+};
+__device__ __forceinline__ Cell3 cell_here() {
+  return Cell3{(int)blockIdx.z, (int)(blockIdx.y * C3_TJ + (threadIdx.x >> 5)),
+               (int)(blockIdx.x * C3_TK + (threadIdx.x & 31))};
 }
 
 // float max via integer atomics (valid for non-negative floats)

@@ -73,7 +73,7 @@ __device__ __forceinline__ float sample_c(const float* __restrict__ f, const flo
   for (int di = 0; di < 2; ++di)
 #pragma unroll
     for (int dj = 0; dj < 2; ++dj) {
-      const long long row = ((long long)I[di] * n1 + J[dj]) * n2;
+      const int row = (I[di] * n1 + J[dj]) * n2;  // face arrays hold < 2^31 entries
       const float wij = wi[di] * wj[dj];
 #pragma unroll
       for (int dk = 0; dk < 2; ++dk) {

@@ -29,16 +29,28 @@ __host__ __device__ inline FaceSpace make_space(int nx, int ny, int nz) {
   return s;
 }
 
-// splits a flat index into (axis, face index, i, j, k); axis 3 = cell
-__device__ __forceinline__ int locate(const FaceSpace& s, long long e, long long* f, int* i, int* j, int* k) {
-  int a = 0;
-  while (a < 3 && e >= s.nf[a]) { e -= s.nf[a]; ++a; }
+// One launch covers the three face arrays (and, with cells, the cell array):
+// blockIdx.z runs over the i-planes of x-faces (nx+1), y-faces (nx), z-faces
+// (nx) and cells (nx); blockIdx.y/x and the thread give j (8 rows) and k (32).
+// Returns the array (0..2 faces, 3 cells) and the element's flat index, or -1
+// outside the array.
+__host__ inline dim3 grid_faces(int nx, int ny, int nz, bool with_cells) {
+  return dim3((unsigned)((nz + 1 + C3_TK - 1) / C3_TK), (unsigned)((ny + 1 + C3_TJ - 1) / C3_TJ),
+              (unsigned)(3 * nx + 1 + (with_cells ? nx : 0)));
+}
+__device__ __forceinline__ int locate(const FaceSpace& s, long long* f, int* i, int* j, int* k) {
+  int z = (int)blockIdx.z, a;
+  if (z < s.nx + 1) a = 0;
+  else if ((z -= s.nx + 1) < s.nx) a = 1;
+  else if ((z -= s.nx) < s.nx) a = 2;
+  else { z -= s.nx; a = 3; }
   const int n1 = s.ny + (a == 1), n2 = s.nz + (a == 2);
-  *f = e;
-  *k = (int)(e % n2);
-  const long long t = e / n2;
-  *j = (int)(t % n1);
-  *i = (int)(t / n1);
+  const int jj = (int)(blockIdx.y * C3_TJ + (threadIdx.x >> 5)), kk = (int)(blockIdx.x * C3_TK + (threadIdx.x & 31));
+  if (jj >= n1 || kk >= n2) return -1;
+  *i = z;
+  *j = jj;
+  *k = kk;
+  *f = ((long long)z * n1 + jj) * n2 + kk;
   return a;
 }
 
@@ -72,19 +84,19 @@ struct PhaseArgs {
   float* beta[3];
 };
 
-__global__ void k_phase_beta(PhaseArgs a) {
+__global__ void __launch_bounds__(C3_NT) k_phase_beta(PhaseArgs a) {
   const FaceSpace& S = a.s;
   const int nx = S.nx, ny = S.ny, nz = S.nz;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < S.total();
-       e += (long long)gridDim.x * blockDim.x) {
+  {
     long long f;
     int i, j, k;
-    const int ax = locate(S, e, &f, &i, &j, &k);
+    const int ax = locate(S, &f, &i, &j, &k);
+    if (ax < 0) return;
     if (ax == 3) {  // cell: pfflip/kernels.py:244-255
       const float phi = phase_field(a.cmass[f], a.rho_min, a.alpha_phi, a.rho_0l);
       a.phi_cell[f] = phi;
       a.is_liq[f] = phi >= 0.5f ? 1 : 0;
-      continue;
+      return;
     }
     // face velocity, pfflip/kernels.py:212-228
     const float m = a.mass[ax][f];
@@ -127,14 +139,13 @@ struct ForceArgs {
 };
 
 // vel_star = vel; vel += g*dt; walls/obstacles zeroed (pfflip/sim.py:176-177, :270-285)
-__global__ void k_save_force(ForceArgs a) {
+__global__ void __launch_bounds__(C3_NT) k_save_force(ForceArgs a) {
   const FaceSpace& S = a.s;
-  const long long nfaces = S.nf[0] + S.nf[1] + S.nf[2];
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nfaces;
-       e += (long long)gridDim.x * blockDim.x) {
+  {
     long long f;
     int i, j, k;
-    const int ax = locate(S, e, &f, &i, &j, &k);
+    const int ax = locate(S, &f, &i, &j, &k);
+    if (ax < 0) return;
     float v = a.vel[ax][f];
     if (a.vstar[ax]) a.vstar[ax][f] = v;
     if (a.g[ax] != 0.f) v += a.g[ax] * a.dt;
@@ -152,14 +163,15 @@ __device__ __forceinline__ float divergence(const float* u, const float* v, cons
 }
 
 // pfflip/kernels.py:338-363
-__global__ void k_build_rhs(int nx, int ny, int nz, const float* __restrict__ u, const float* __restrict__ v,
-                            const float* __restrict__ w, const float* __restrict__ wsum, float* __restrict__ b,
-                            float dx, float dt, float rho_0, float k_div) {
-  const long long n = (long long)nx * ny * nz;
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(c % nz);
-    const long long t = c / nz;
-    const int j = (int)(t % ny), i = (int)(t / ny);
+__global__ void __launch_bounds__(C3_NT) k_build_rhs(int nx, int ny, int nz, const float* __restrict__ u,
+                                                    const float* __restrict__ v, const float* __restrict__ w,
+                                                    const float* __restrict__ wsum, float* __restrict__ b, float dx,
+                                                    float dt, float rho_0, float k_div) {
+  const Cell3 cc = cell_here();
+  if (cc.j >= ny || cc.k >= nz) return;
+  {
+    const int i = cc.i, j = cc.j, k = cc.k;
+    const long long c = ((long long)i * ny + j) * nz + k;
     const float du = divergence(u, v, w, i, j, k, nx, ny, nz);
     float rhs = -(dx / dt) * du;
     if (k_div > 0.f) {
@@ -179,19 +191,18 @@ struct ProjArgs {
 };
 
 // pfflip/kernels.py:366-387
-__global__ void k_project(ProjArgs a) {
+__global__ void __launch_bounds__(C3_NT) k_project(ProjArgs a) {
   const FaceSpace& S = a.s;
-  const long long nfaces = S.nf[0] + S.nf[1] + S.nf[2];
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nfaces;
-       e += (long long)gridDim.x * blockDim.x) {
+  {
     long long f;
     int i, j, k;
-    const int ax = locate(S, e, &f, &i, &j, &k);
+    const int ax = locate(S, &f, &i, &j, &k);
+    if (ax < 0) return;
     const float bc = a.beta[ax][f];
-    if (bc == 0.f) continue;
+    if (bc == 0.f) return;
     const int im = i - (ax == 0), jm = j - (ax == 1), km = k - (ax == 2);
-    if (im < 0 || jm < 0 || km < 0) continue;
-    if (i >= S.nx || j >= S.ny || k >= S.nz) continue;
+    if (im < 0 || jm < 0 || km < 0) return;
+    if (i >= S.nx || j >= S.ny || k >= S.nz) return;
     const float pi = a.p[((long long)i * S.ny + j) * S.nz + k];
     const float pm = a.p[((long long)im * S.ny + jm) * S.nz + km];
     a.vel[ax][f] -= a.dt * bc * (pi - pm) / a.dx;
@@ -203,15 +214,12 @@ __global__ void __launch_bounds__(256) k_max_div(int nx, int ny, int nz, const f
                                                  const float* __restrict__ v, const float* __restrict__ w, float dx,
                                                  float* out) {
   __shared__ float sh[40];
-  const long long n = (long long)nx * ny * nz;
+  const Cell3 cc = cell_here();
   float m = 0.f;
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(c % nz);
-    const long long t = c / nz;
-    const int j = (int)(t % ny), i = (int)(t / ny);
-    const float d = divergence(u, v, w, i, j, k, nx, ny, nz);
+  if (cc.j < ny && cc.k < nz) {
+    const float d = divergence(u, v, w, cc.i, cc.j, cc.k, nx, ny, nz);
     const float q = fabsf(d / dx);
-    m = fmaxf(m, isnan(q) ? INFINITY : q);
+    m = isnan(q) ? INFINITY : q;
   }
   m = block_max<256>(m, sh);
   if (threadIdx.x == 0) atomic_max_nonneg(out, m);
@@ -228,13 +236,14 @@ __global__ void __launch_bounds__(256) k_max_div(int nx, int ny, int nz, const f
 constexpr int EX_TI = 4, EX_TJ = 8, EX_TK = 32, EX_NT = 256;
 enum : unsigned char { EX_UNKNOWN = 0, EX_KNOWN = 1, EX_ABSENT = 2 };
 
-__global__ void __launch_bounds__(EX_NT) k_extrapolate(int nx, int ny, int nz, int ax, int H,
+template <int H>
+__global__ void __launch_bounds__(EX_NT) k_extrapolate(int nx, int ny, int nz, int ax,
                                                        const float* __restrict__ vel, const int* __restrict__ is_liq,
                                                        float* __restrict__ vel_liq, int* __restrict__ known_out) {
   extern __shared__ __align__(16) unsigned char exsm[];
   const int n0 = nx + (ax == 0), n1 = ny + (ax == 1), n2 = nz + (ax == 2);
-  const int R0 = EX_TI + 2 * H, R1 = EX_TJ + 2 * H, R2 = EX_TK + 2 * H;
-  const int RN = R0 * R1 * R2;
+  constexpr int R0 = EX_TI + 2 * H, R1 = EX_TJ + 2 * H, R2 = EX_TK + 2 * H;
+  constexpr int RN = R0 * R1 * R2;
   float* V0 = reinterpret_cast<float*>(exsm);
   float* V1 = V0 + RN;
   unsigned char* K0 = reinterpret_cast<unsigned char*>(V1 + RN);
@@ -350,8 +359,7 @@ int pf_phase_beta(const pf_grid* g, const float* mass_x, const float* mass_y, co
   a.phi_cell = phi_cell; a.is_liq = is_liquid;
   a.phi_face[0] = phi_face_x; a.phi_face[1] = phi_face_y; a.phi_face[2] = phi_face_z;
   a.beta[0] = beta_x; a.beta[1] = beta_y; a.beta[2] = beta_z;
-  const long long tot = a.s.nf[0] + a.s.nf[1] + a.s.nf[2] + a.s.nc;
-  k_phase_beta<<<ew_blocks(tot), 256, 0, S(stream)>>>(a);
+  k_phase_beta<<<grid_faces(g->nx, g->ny, g->nz, true), C3_NT, 0, S(stream)>>>(a);
   PF_LAUNCHED();
   return PF_OK;
 }
@@ -367,7 +375,7 @@ int pf_save_and_force(const pf_grid* g, float* vel_x, float* vel_y, float* vel_z
   a.solid = solid;
   a.g[0] = gx; a.g[1] = gy; a.g[2] = gz;
   a.dt = dt;
-  k_save_force<<<ew_blocks(a.s.nf[0] + a.s.nf[1] + a.s.nf[2]), 256, 0, S(stream)>>>(a);
+  k_save_force<<<grid_faces(g->nx, g->ny, g->nz, false), C3_NT, 0, S(stream)>>>(a);
   PF_LAUNCHED();
   return PF_OK;
 }
@@ -377,8 +385,9 @@ int pf_build_rhs(const pf_grid* g, const float* vel_x, const float* vel_y, const
   PF_REQUIRE(g && vel_x && vel_y && vel_z && b, "null argument");
   PF_REQUIRE(k_div <= 0.f || cell_wsum, "cell_wsum required when k_div > 0");
   const long long n = (long long)g->nx * g->ny * g->nz;
-  k_build_rhs<<<ew_blocks(n), 256, 0, S(stream)>>>(g->nx, g->ny, g->nz, vel_x, vel_y, vel_z, cell_wsum, b, g->dx, dt,
-                                                   rho_0, k_div);
+  (void)n;
+  k_build_rhs<<<grid_cells(g->nx, g->ny, g->nz), C3_NT, 0, S(stream)>>>(g->nx, g->ny, g->nz, vel_x, vel_y, vel_z,
+                                                                        cell_wsum, b, g->dx, dt, rho_0, k_div);
   PF_LAUNCHED();
   return PF_OK;
 }
@@ -393,7 +402,7 @@ int pf_project(const pf_grid* g, const float* p, const float* beta_x, const floa
   a.vel[0] = vel_x; a.vel[1] = vel_y; a.vel[2] = vel_z;
   a.dx = g->dx;
   a.dt = dt;
-  k_project<<<ew_blocks(a.s.nf[0] + a.s.nf[1] + a.s.nf[2]), 256, 0, S(stream)>>>(a);
+  k_project<<<grid_faces(g->nx, g->ny, g->nz, false), C3_NT, 0, S(stream)>>>(a);
   PF_LAUNCHED();
   return PF_OK;
 }
@@ -404,7 +413,8 @@ int pf_max_divergence(const pf_grid* g, const float* vel_x, const float* vel_y, 
   cudaStream_t s = S(stream);
   PF_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float), s));
   const long long n = (long long)g->nx * g->ny * g->nz;
-  k_max_div<<<ew_blocks(n), 256, 0, s>>>(g->nx, g->ny, g->nz, vel_x, vel_y, vel_z, g->dx, out);
+  (void)n;
+  k_max_div<<<grid_cells(g->nx, g->ny, g->nz), C3_NT, 0, s>>>(g->nx, g->ny, g->nz, vel_x, vel_y, vel_z, g->dx, out);
   PF_LAUNCHED();
   return PF_OK;
 }
@@ -422,14 +432,24 @@ int pf_extrapolate(const pf_grid* g, const float* vel_x, const float* vel_y, con
   const size_t smem = rn * (2 * sizeof(float) + 2);
   static int attr_done = 0;
   if (!attr_done) {
-    PF_CUDA_TRY(cudaFuncSetAttribute(k_extrapolate, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    PF_CUDA_TRY(cudaFuncSetAttribute(k_extrapolate<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    PF_CUDA_TRY(cudaFuncSetAttribute(k_extrapolate<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    PF_CUDA_TRY(cudaFuncSetAttribute(k_extrapolate<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    PF_CUDA_TRY(cudaFuncSetAttribute(k_extrapolate<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    PF_CUDA_TRY(cudaFuncSetAttribute(k_extrapolate<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
     attr_done = 1;
   }
   for (int ax = 0; ax < 3; ++ax) {
     const int n0 = g->nx + (ax == 0), n1 = g->ny + (ax == 1), n2 = g->nz + (ax == 2);
     dim3 grid((n2 + EX_TK - 1) / EX_TK, (n1 + EX_TJ - 1) / EX_TJ, (n0 + EX_TI - 1) / EX_TI);
-    k_extrapolate<<<grid, EX_NT, smem, S(stream)>>>(g->nx, g->ny, g->nz, ax, H, vin[ax], is_liquid, vout[ax],
-                                                    kout[ax]);
+    cudaStream_t st = S(stream);
+    switch (H) {
+      case 0: k_extrapolate<0><<<grid, EX_NT, smem, st>>>(g->nx, g->ny, g->nz, ax, vin[ax], is_liquid, vout[ax], kout[ax]); break;
+      case 1: k_extrapolate<1><<<grid, EX_NT, smem, st>>>(g->nx, g->ny, g->nz, ax, vin[ax], is_liquid, vout[ax], kout[ax]); break;
+      case 2: k_extrapolate<2><<<grid, EX_NT, smem, st>>>(g->nx, g->ny, g->nz, ax, vin[ax], is_liquid, vout[ax], kout[ax]); break;
+      case 3: k_extrapolate<3><<<grid, EX_NT, smem, st>>>(g->nx, g->ny, g->nz, ax, vin[ax], is_liquid, vout[ax], kout[ax]); break;
+      default: k_extrapolate<4><<<grid, EX_NT, smem, st>>>(g->nx, g->ny, g->nz, ax, vin[ax], is_liquid, vout[ax], kout[ax]); break;
+    }
     PF_LAUNCHED();
   }
   return PF_OK;

@@ -102,16 +102,13 @@ __device__ __forceinline__ float apply_row(const float* __restrict__ p, const fl
   return d * pc - s;
 }
 
-__global__ void k_apply_A(int nx, int ny, int nz, const float* __restrict__ p, const float* __restrict__ bx,
-                          const float* __restrict__ by, const float* __restrict__ bz, const float* __restrict__ diag,
-                          float* __restrict__ out, int flux) {
-  const long long n = (long long)nx * ny * nz;
-  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(c % nz);
-    const long long t = c / nz;
-    const int j = (int)(t % ny), i = (int)(t / ny);
-    out[c] = apply_row(p, bx, by, bz, diag, nx, ny, nz, i, j, k, flux);
-  }
+__global__ void __launch_bounds__(C3_NT) k_apply_A(int nx, int ny, int nz, const float* __restrict__ p,
+                                                  const float* __restrict__ bx, const float* __restrict__ by,
+                                                  const float* __restrict__ bz, const float* __restrict__ diag,
+                                                  float* __restrict__ out, int flux) {
+  const Cell3 c = cell_here();
+  if (c.j >= ny || c.k >= nz) return;
+  out[((long long)c.i * ny + c.j) * nz + c.k] = apply_row(p, bx, by, bz, diag, nx, ny, nz, c.i, c.j, c.k, flux);
 }
 
 // --------------------------------------------------------------- hierarchy build
@@ -410,7 +407,7 @@ __global__ void __launch_bounds__(SW_NT) k_rb_tile(SweepArgs<T, TB> a) {
     if (s_last) {
       __threadfence();
       double v = 0.0;
-      for (int q = tid; q < nb; q += SW_NT) v += ((volatile double*)a.partials)[q];
+      for (int q = tid; q < nb; q += SW_NT) v += __ldcg(a.partials + q);
       v = block_sum<SW_NT>(v, sred);
       if (tid == 0) {
         a.st->sum_last = v;
@@ -598,7 +595,7 @@ __global__ void __launch_bounds__(SW_NT) k_rb_tile_tma(const __grid_constant__ T
     if (s_last) {
       __threadfence();
       double v = 0.0;
-      for (int q = tid; q < nb; q += SW_NT) v += ((volatile double*)a.partials)[q];
+      for (int q = tid; q < nb; q += SW_NT) v += __ldcg(a.partials + q);
       v = block_sum<SW_NT>(v, sred);
       if (tid == 0) {
         a.st->sum_last = v;
@@ -617,14 +614,14 @@ __global__ void k_residual_restrict(int n0, int n1, int n2, const T* __restrict_
                                     const T* __restrict__ bz, T* __restrict__ cb, float rscale, float* fine_r,
                                     const MGState* st, int flux) {
   if (is_done(st)) return;
-  const int C0 = n0 >> 1, C1 = n1 >> 1, C2 = n2 >> 1;
-  const long long nc = (long long)C0 * C1 * C2;
+  const int C1 = n1 >> 1, C2 = n2 >> 1;
   const float bsc = b_scale ? *b_scale : 1.f;
   const long long sI = (long long)n1 * n2;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nc; e += (long long)gridDim.x * blockDim.x) {
-    const int K = (int)(e % C2);
-    const long long t = e / C2;
-    const int J = (int)(t % C1), I = (int)(t / C1);
+  {
+    const Cell3 cc3 = cell_here();
+    const int I = cc3.i, J = cc3.j, K = cc3.k;
+    if (J >= C1 || K >= C2) return;
+    const long long e = ((long long)I * C1 + J) * C2 + K;
     float acc = 0.f;
 #pragma unroll
     for (int aa = 0; aa < 2; ++aa)
@@ -764,7 +761,14 @@ __device__ __forceinline__ void bt_half_sweep(const BottomLevel& L, R* P, const 
                                               const float* Y, const float* Z, int color, R omega, int flux, int tid,
                                               int nt) {
   const int n0 = L.n0, n1 = L.n1, n2 = L.n2;
-  if ((n2 & 1) == 0) {  // only the cells of this colour: two per pair along k
+  if (L.s1 >= 0 && n2 >= 2) {  // powers of two: only the cells of this colour, shift indexing
+    const int hn = (n0 * n1 * n2) >> 1, sh = L.s2 - 1, hm = (n2 >> 1) - 1;
+    for (int e = tid; e < hn; e += nt) {
+      const int h = e & hm, row = e >> sh, j = row & (n1 - 1), i = row >> L.s1;
+      const int k = 2 * h + ((color - i - j) & 1);
+      bt_relax<R>(P, B, X, Y, Z, n0, n1, n2, i, j, k, omega, flux);
+    }
+  } else if ((n2 & 1) == 0) {  // only the cells of this colour: two per pair along k
     const int hn = (n0 * n1 * n2) >> 1, hk = n2 >> 1;
     for (int e = tid; e < hn; e += nt) {
       const int h = e % hk, row = e / hk, j = row % n1, i = row / n1;
@@ -861,8 +865,20 @@ __global__ void __launch_bounds__(BT_NT) k_bottom(BottomArgs<T, TB> a) {
     const int C1 = n1 >> 1, C2 = n2 >> 1, nc = (n0 >> 1) * C1 * C2;
     float* Bc = ptrs(l + 1).B;
     const int sI = n1 * n2;
+    const bool p2 = L.s1 >= 1 && L.s2 >= 1;
     for (int ec = tid; ec < nc; ec += BT_NT) {
-      const int K = ec % C2, t = ec / C2, J = t % C1, I = t / C1;
+      int I, J, K;
+      if (p2) {
+        K = ec & (C2 - 1);
+        const int t = ec >> (L.s2 - 1);
+        J = t & (C1 - 1);
+        I = t >> (L.s1 - 1);
+      } else {
+        K = ec % C2;
+        const int t = ec / C2;
+        J = t % C1;
+        I = t / C1;
+      }
       float acc = 0.f;
 #pragma unroll
       for (int aa = 0; aa < 2; ++aa)
@@ -1025,6 +1041,22 @@ __device__ __forceinline__ float zval(const T* p, long long e, float zs, float c
   return ldT(p + e) * zs + c;
 }
 
+// 4-wide loads/stores of the CG vectors (16-byte float4, 8-byte 16-bit quads)
+__device__ __forceinline__ float4 ld4(const float* p, long long i4) { return reinterpret_cast<const float4*>(p)[i4]; }
+__device__ __forceinline__ float4 ld4(const __half* p, long long i4) {
+  const uint2 u = reinterpret_cast<const uint2*>(p)[i4];
+  const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+  const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+  return make_float4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ float4 ld4(const __nv_bfloat16* p, long long i4) {
+  const uint2 u = reinterpret_cast<const uint2*>(p)[i4];
+  const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
+  const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+  return make_float4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ void st4(float* p, long long i4, float4 v) { reinterpret_cast<float4*>(p)[i4] = v; }
+
 // q = z; rz = <r, z>   (pfflip/poisson.py:378-380)
 template <class T>
 __global__ void __launch_bounds__(RED_NT) k_init_q(long long n, const T* __restrict__ p, const float* __restrict__ r,
@@ -1047,26 +1079,29 @@ __global__ void __launch_bounds__(RED_NT) k_init_q(long long n, const T* __restr
 
 // Ap = A q; qAq = <q, Ap>; it += 1; alpha = rz/qAq or stop when qAq <= 0
 // (pfflip/poisson.py:384-389)
-__global__ void __launch_bounds__(RED_NT) k_apply_dot(int nx, int ny, int nz, const float* __restrict__ q,
-                                                      const float* __restrict__ bx, const float* __restrict__ by,
-                                                      const float* __restrict__ bz, const float* __restrict__ diag,
-                                                      float* __restrict__ Ap, double* partials, unsigned* counter,
-                                                      MGState* st, int flux) {
+__global__ void __launch_bounds__(C3_NT) k_apply_dot(int nx, int ny, int nz, const float* __restrict__ q,
+                                                     const float* __restrict__ bx, const float* __restrict__ by,
+                                                     const float* __restrict__ bz, const float* __restrict__ diag,
+                                                     float* __restrict__ Ap, double* partials, unsigned* counter,
+                                                     MGState* st, int flux) {
   if (is_done(st)) return;
   __shared__ double sh[40];
-  const long long n = (long long)nx * ny * nz;
+  const Cell3 c = cell_here();  // blockIdx.z counts groups of 4 i-planes
   double s = 0.0;
-  for (long long c = blockIdx.x * (long long)RED_NT + threadIdx.x; c < n; c += (long long)gridDim.x * RED_NT) {
-    const int k = (int)(c % nz);
-    const long long t = c / nz;
-    const int j = (int)(t % ny), i = (int)(t / ny);
-    const float v = apply_row(q, bx, by, bz, diag, nx, ny, nz, i, j, k, flux);
-    Ap[c] = v;
-    s += (double)q[c] * (double)v;
+  if (c.j < ny && c.k < nz) {
+#pragma unroll
+    for (int di = 0; di < 4; ++di) {
+      const int i = 4 * c.i + di;
+      if (i >= nx) break;
+      const long long e = ((long long)i * ny + c.j) * nz + c.k;
+      const float v = apply_row(q, bx, by, bz, diag, nx, ny, nz, i, c.j, c.k, flux);
+      Ap[e] = v;
+      s += (double)q[e] * (double)v;
+    }
   }
-  s = block_sum<RED_NT>(s, sh);
+  s = block_sum<C3_NT>(s, sh);
   double tot;
-  if (grid_sum_last<RED_NT>(s, partials, counter, &tot, sh) && threadIdx.x == 0) {
+  if (grid_sum_last<C3_NT>(s, partials, counter, &tot, sh) && threadIdx.x == 0) {
     st->it += 1;
     st->qAq = tot;
     if (!(tot > 0.0)) {
@@ -1081,7 +1116,7 @@ __global__ void __launch_bounds__(RED_NT) k_apply_dot(int nx, int ny, int nz, co
 }
 
 // x += alpha q; r_new = r - alpha Ap (r kept as r_prev); rel = max|r_new|/bnorm
-// (pfflip/poisson.py:390-398)
+// (pfflip/poisson.py:390-398).  4-wide, grid-stride.
 __global__ void __launch_bounds__(RED_NT) k_update_xr(long long n, const float* __restrict__ q,
                                                       const float* __restrict__ Ap, const float* __restrict__ r,
                                                       float* __restrict__ r_new, float* __restrict__ x,
@@ -1090,11 +1125,27 @@ __global__ void __launch_bounds__(RED_NT) k_update_xr(long long n, const float* 
   __shared__ float shf[40];
   const float af = st->alpha_f, naf = st->neg_alpha_f;
   float m = 0.f;
-  for (long long e = blockIdx.x * (long long)RED_NT + threadIdx.x; e < n; e += (long long)gridDim.x * RED_NT) {
-    x[e] += af * q[e];
-    const float v = r[e] + naf * Ap[e];
-    r_new[e] = v;
-    m = fmaxf(m, isfinite(v) ? fabsf(v) : INFINITY);
+  const long long n4 = n >> 2, stride = (long long)gridDim.x * RED_NT;
+  auto one = [&](float qv, float av, float rv, float& xv, float& rn) {
+    xv += af * qv;
+    rn = rv + naf * av;
+    m = fmaxf(m, isfinite(rn) ? fabsf(rn) : INFINITY);
+  };
+  for (long long i = blockIdx.x * (long long)RED_NT + threadIdx.x; i < n4; i += stride) {
+    const float4 qv = ld4(q, i), av = ld4(Ap, i), rv = ld4(r, i);
+    float4 xv = ld4(x, i), rn;
+    one(qv.x, av.x, rv.x, xv.x, rn.x);
+    one(qv.y, av.y, rv.y, xv.y, rn.y);
+    one(qv.z, av.z, rv.z, xv.z, rn.z);
+    one(qv.w, av.w, rv.w, xv.w, rn.w);
+    st4(x, i, xv);
+    st4(r_new, i, rn);
+  }
+  for (long long e = 4 * n4 + blockIdx.x * (long long)RED_NT + threadIdx.x; e < n; e += stride) {
+    float xv = x[e], rn;
+    one(q[e], Ap[e], r[e], xv, rn);
+    x[e] = xv;
+    r_new[e] = rn;
   }
   m = block_max<RED_NT>(m, shf);
   float tot;
@@ -1116,7 +1167,7 @@ __global__ void __launch_bounds__(RED_NT) k_update_xr(long long n, const float* 
 }
 
 // rz_new = <r, z>, rpz = <r_prev, z>, beta = max((rz_new - rpz)/rz, 0), rz = rz_new
-// (pfflip/poisson.py:402-406)
+// (pfflip/poisson.py:402-406).  4-wide, grid-stride.
 template <class T>
 __global__ void __launch_bounds__(RED_NT) k_dots(long long n, const T* __restrict__ p, const float* __restrict__ r,
                                                  const float* __restrict__ r_prev, double* partials,
@@ -1125,11 +1176,21 @@ __global__ void __launch_bounds__(RED_NT) k_dots(long long n, const T* __restric
   __shared__ double sh[40];
   const float c = st->c_shift, zs = mixed ? st->zscale : 1.f;
   double s1 = 0.0, s2 = 0.0;
-  for (long long e = blockIdx.x * (long long)RED_NT + threadIdx.x; e < n; e += (long long)gridDim.x * RED_NT) {
-    const double z = (double)zval(p, e, zs, c);
-    s1 += (double)r[e] * z;
-    s2 += (double)r_prev[e] * z;
+  const long long n4 = n >> 2, stride = (long long)gridDim.x * RED_NT;
+  auto one = [&](float pv, float rv, float qv) {
+    const double z = (double)(pv * zs + c);
+    s1 += (double)rv * z;
+    s2 += (double)qv * z;
+  };
+  for (long long i = blockIdx.x * (long long)RED_NT + threadIdx.x; i < n4; i += stride) {
+    const float4 pv = ld4(p, i), rv = ld4(r, i), qv = ld4(r_prev, i);
+    one(pv.x, rv.x, qv.x);
+    one(pv.y, rv.y, qv.y);
+    one(pv.z, rv.z, qv.z);
+    one(pv.w, rv.w, qv.w);
   }
+  for (long long e = 4 * n4 + blockIdx.x * (long long)RED_NT + threadIdx.x; e < n; e += stride)
+    one(ldT(p + e), r[e], r_prev[e]);
   s1 = block_sum<RED_NT>(s1, sh);
   s2 = block_sum<RED_NT>(s2, sh);
   double t1, t2;
@@ -1144,13 +1205,23 @@ __global__ void __launch_bounds__(RED_NT) k_dots(long long n, const T* __restric
   }
 }
 
-// q = z + beta q   (pfflip/poisson.py:405, scale_add)
+// q = z + beta q   (pfflip/poisson.py:405, scale_add).  4-wide, grid-stride.
 template <class T>
 __global__ void __launch_bounds__(RED_NT) k_update_q(long long n, const T* __restrict__ p, float* __restrict__ q,
                                                      MGState* st, int mixed) {
   if (is_done(st)) return;
   const float c = st->c_shift, zs = mixed ? st->zscale : 1.f, bf = st->beta_f;
-  for (long long e = blockIdx.x * (long long)RED_NT + threadIdx.x; e < n; e += (long long)gridDim.x * RED_NT)
+  const long long n4 = n >> 2, stride = (long long)gridDim.x * RED_NT;
+  for (long long i = blockIdx.x * (long long)RED_NT + threadIdx.x; i < n4; i += stride) {
+    const float4 pv = ld4(p, i);
+    float4 qv = ld4(q, i);
+    qv.x = (pv.x * zs + c) + bf * qv.x;
+    qv.y = (pv.y * zs + c) + bf * qv.y;
+    qv.z = (pv.z * zs + c) + bf * qv.z;
+    qv.w = (pv.w * zs + c) + bf * qv.w;
+    st4(q, i, qv);
+  }
+  for (long long e = 4 * n4 + blockIdx.x * (long long)RED_NT + threadIdx.x; e < n; e += stride)
     q[e] = zval(p, e, zs, c) + bf * q[e];
 }
 
@@ -1292,6 +1363,8 @@ template <class T> LV<T> view(pf_mg_plan* P, int lv) {
 
 // one thread per element: every load of a thread is independent of the others
 int red_grid(long long n) { return grid_for(n, RED_NT, (int)(pf::kPartials / 2)); }
+// 4-wide grid-stride kernels: about 8 CTAs per SM
+int vec_grid(long long n) { return grid_for((n + 3) / 4, RED_NT, kNumSMs * 8); }
 int ew_grid(long long n) { return grid_for(n, 256, 1 << 20); }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
@@ -1474,8 +1547,8 @@ int vcycle(pf_mg_plan* P, int lv, const TB* b, const float* b_scale, bool want_m
   }
   LV<T> C = view<T>(P, lv + 1);
   const pf_mg_level& CL = P->d.lev[lv + 1];
-  k_residual_restrict<T, TB><<<ew_grid(ncells(CL)), 256, 0, s>>>(L.nx, L.ny, L.nz, cur, b, b_scale, V.bx, V.by,
-                                                                V.bz, C.b, rscale, nullptr, ST(P), FLUX(P));
+  k_residual_restrict<T, TB><<<grid_cells(CL.nx, CL.ny, CL.nz), C3_NT, 0, s>>>(
+      L.nx, L.ny, L.nz, cur, b, b_scale, V.bx, V.by, V.bz, C.b, rscale, nullptr, ST(P), FLUX(P));
   PF_LAUNCHED();
   T* pc = nullptr;
   PF_TRY((vcycle<T, T>(P, lv + 1, C.b, nullptr, false, s, &pc)));
@@ -1530,10 +1603,11 @@ template <class T> int enqueue_iteration(pf_mg_plan* P, int par, cudaStream_t s)
   const long long n = ncells(L0);
   float* r_cur = par ? P->d.res_alt : P->d.res_v;
   float* r_new = par ? P->d.res_v : P->d.res_alt;
-  k_apply_dot<<<red_grid(n), RED_NT, 0, s>>>(L0.nx, L0.ny, L0.nz, P->d.q, L0.bx, L0.by, L0.bz, nullptr, P->d.Ap,
-                                             P->d.partials, CNT(P, CNT_APPLY_DOT), ST(P), FLUX(P));
+  k_apply_dot<<<grid_cells((L0.nx + 3) / 4, L0.ny, L0.nz), C3_NT, 0, s>>>(L0.nx, L0.ny, L0.nz, P->d.q, L0.bx, L0.by, L0.bz,
+                                                                nullptr, P->d.Ap, P->d.partials,
+                                                                CNT(P, CNT_APPLY_DOT), ST(P), FLUX(P));
   PF_LAUNCHED();
-  k_update_xr<<<red_grid(n), RED_NT, 0, s>>>(n, P->d.q, P->d.Ap, r_cur, r_new, P->d.x, P->d.partials,
+  k_update_xr<<<vec_grid(n), RED_NT, 0, s>>>(n, P->d.q, P->d.Ap, r_cur, r_new, P->d.x, P->d.partials,
                                              CNT(P, CNT_UPDATE_XR), ST(P));
   PF_LAUNCHED();
   if (mixed(P)) {
@@ -1542,10 +1616,10 @@ template <class T> int enqueue_iteration(pf_mg_plan* P, int par, cudaStream_t s)
   }
   T* p0 = nullptr;
   PF_TRY(vcycle0<T>(P, r_new, s, &p0));
-  k_dots<T><<<red_grid(n), RED_NT, 0, s>>>(n, p0, r_new, r_cur, P->d.partials, CNT(P, CNT_DOTS), ST(P),
+  k_dots<T><<<vec_grid(n), RED_NT, 0, s>>>(n, p0, r_new, r_cur, P->d.partials, CNT(P, CNT_DOTS), ST(P),
                                            mixed(P) ? 1 : 0);
   PF_LAUNCHED();
-  k_update_q<T><<<ew_grid(n), RED_NT, 0, s>>>(n, p0, P->d.q, ST(P), mixed(P) ? 1 : 0);
+  k_update_q<T><<<vec_grid(n), RED_NT, 0, s>>>(n, p0, P->d.q, ST(P), mixed(P) ? 1 : 0);
   PF_LAUNCHED();
   return PF_OK;
 }
@@ -1857,8 +1931,8 @@ int pf_apply_A(const pf_grid* g, const float* p, const float* bx, const float* b
   PF_REQUIRE(g && p && bx && by && bz && out, "null argument");
   PF_REQUIRE(stencil == PF_STENCIL_REFERENCE || stencil == PF_STENCIL_FLUX, "bad stencil");
   const long long n = (long long)g->nx * g->ny * g->nz;
-  k_apply_A<<<ew_grid(n), 256, 0, S(stream)>>>(g->nx, g->ny, g->nz, p, bx, by, bz, diag, out,
-                                               stencil == PF_STENCIL_FLUX ? 1 : 0);
+  k_apply_A<<<grid_cells(g->nx, g->ny, g->nz), C3_NT, 0, S(stream)>>>(g->nx, g->ny, g->nz, p, bx, by, bz, diag, out,
+                                                                      stencil == PF_STENCIL_FLUX ? 1 : 0);
   PF_LAUNCHED();
   return PF_OK;
 }

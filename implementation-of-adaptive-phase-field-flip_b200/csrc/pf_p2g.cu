@@ -141,16 +141,22 @@ __device__ __forceinline__ void p2g_grid(const P2GArgs& a, float* acc, int i, in
                                          int lj, int lane) {
   Box<G> box;
   box.zero();
+  // one particle of prefetch: the loads of t+1 are in flight while t is splatted
+  float4 Pn = make_float4(0.f, 0.f, 0.f, 0.f), Vn = Pn;
+  if (s < e) {
+    Pn = __ldg(a.pos + s);
+    if (G < 3) Vn = __ldg(a.vel + s);
+  }
   for (int t = s; t < e; ++t) {
-    const float4 P = __ldg(a.pos + t);
+    const float4 P = Pn, V = Vn;
+    if (t + 1 < e) {
+      Pn = __ldg(a.pos + t + 1);
+      if (G < 3) Vn = __ldg(a.vel + t + 1);
+    }
     const int flags = __float_as_int(P.w);
     if ((flags >> PF_PSTATE_SHIFT) & 3) continue;  // droplets / dead particles do not splat
     const float mp = (flags & PF_FLAG_LIQUID) ? a.rho_l : a.rho_g;
-    float up = 0.f;
-    if (G < 3) {
-      const float4 V = __ldg(a.vel + t);
-      up = G == 0 ? V.x : G == 1 ? V.y : V.z;
-    }
+    const float up = G == 0 ? V.x : G == 1 ? V.y : V.z;
     const float x[3] = {P.x, P.y, P.z};
     box.add(i, j, k, x, mp, up, a.dx, a.inv_r2);
   }
