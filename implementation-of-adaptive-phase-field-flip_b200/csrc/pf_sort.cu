@@ -241,3 +241,118 @@ int pf_sort_particles(const pf_grid* g, int64_t n, const float* pos4_in, const f
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- sort without a workspace
+// pf_sort_particles_static: the same stable sort for hosts that cannot hand
+// the library a device workspace.  Some hosts fix all device memory when they
+// start (one pool, sized once, with no allocator reachable from the step) or
+// embed the step in code that must not allocate at all; such callers own the
+// particle streams and the outputs, and nothing else.
+//
+// Scratch: the keys and arrival ranks of pass 1 sit in pos4_out (8 of its 16
+// bytes per particle) until the gather overwrites it; the slot of a particle
+// is cell_start[key] + rank, so no per-cell cursor copy is needed.  The only
+// scratch left is the scan's per-tile sums, held in a file-scope device array
+// sized for grids of up to kStaticMaxCells cells.  Nothing in that array has
+// to start at zero: k_scan_tiles writes every entry the later passes read.
+// The counts accumulate in cell_start, which each call clears on its stream.
+// All calls on one device share the array, so calls whose executions overlap
+// (two streams, two host threads) race on it.
+namespace pf {
+
+constexpr long long kStaticMaxCells = PF_SORT_STATIC_MAX_CELLS;
+constexpr int kStaticTiles = (int)((kStaticMaxCells + 1 + SCAN_TILE - 1) / SCAN_TILE);
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) int g_static_tile_sums[(kStaticTiles + 63) / 64 * 64];
+
+// device address of g_static_tile_sums, looked up once per device
+static std::atomic<int*> g_static_sums_addr[kMaxDevices];
+
+static int static_tile_sums(int** out) {
+  int dev = 0;
+  PF_CUDA_TRY(cudaGetDevice(&dev));
+  PF_REQUIRE(dev >= 0 && dev < kMaxDevices, "device ordinal %d beyond %d", dev, kMaxDevices);
+  int* a = g_static_sums_addr[dev].load(std::memory_order_acquire);
+  if (!a) {
+    void* sym = nullptr;
+    PF_CUDA_TRY(cudaGetSymbolAddress(&sym, g_static_tile_sums));
+    a = static_cast<int*>(sym);
+    g_static_sums_addr[dev].store(a, std::memory_order_release);
+  }
+  *out = a;
+  return PF_OK;
+}
+
+// pass 1: key and arrival rank within the cell (ranks of one cell are
+// 0..count-1 in some order), counts into `counts`
+__global__ void k_keys_rank(long long n, const float4* __restrict__ pos, float dx, int nx, int ny, int nz,
+                            int2* __restrict__ key_rank, int* __restrict__ counts) {
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
+    const long long p = base + threadIdx.x;
+    const bool in = p < n;
+    const unsigned active = __ballot_sync(0xffffffffu, in);
+    if (!in) continue;
+    const float4 q = __ldg(pos + p);
+    const int key = cell_key(q.x, q.y, q.z, dx, nx, ny, nz);
+    key_rank[p] = make_int2(key, agg_inc(counts, key, active));
+  }
+}
+
+// pass 3: perm[start[key] + rank] = p; the slots of one cell are then in
+// arrival order, which k_fix_order turns into index order
+__global__ void k_scatter_rank(long long n, const int2* __restrict__ key_rank, const int* __restrict__ start,
+                               int* __restrict__ perm) {
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    const int2 kr = key_rank[p];
+    perm[start[kr.x] + kr.y] = (int)p;
+  }
+}
+
+}  // namespace pf
+
+extern "C" int pf_sort_particles_static(const pf_grid* g, int64_t n, const float* pos4_in, const float* vel4_in,
+                                        float* pos4_out, float* vel4_out, int32_t* keys_out, int32_t* perm_out,
+                                        int32_t* cell_start, void* stream) {
+  PF_REQUIRE(g && n >= 0 && pos4_in && vel4_in && pos4_out && vel4_out && keys_out && perm_out && cell_start,
+             "null argument");
+  PF_REQUIRE(g->nx > 0 && g->ny > 0 && g->nz > 0 && g->dx > 0.f, "bad grid");
+  const long long nc = (long long)g->nx * g->ny * g->nz;
+  PF_REQUIRE(nc <= kStaticMaxCells,
+             "grid of %lld cells exceeds the %lld cells (512^3) the static scratch covers; use pf_sort_particles "
+             "with a workspace",
+             nc, kStaticMaxCells);
+  PF_REQUIRE(n < (1LL << 31), "too large for int32 indices");
+  PF_REQUIRE(aligned16(pos4_in) && aligned16(vel4_in) && aligned16(pos4_out) && aligned16(vel4_out),
+             "particle streams must be 16-byte aligned");
+  PF_REQUIRE(pos4_in != pos4_out && vel4_in != vel4_out, "sort output must not alias its input");
+  int* sums = nullptr;
+  const int rc = static_tile_sums(&sums);
+  if (rc != PF_OK) return rc;
+  cudaStream_t s = S(stream);
+  const long long tiles = (nc + 1 + SCAN_TILE - 1) / SCAN_TILE;
+  int2* key_rank = reinterpret_cast<int2*>(pos4_out);
+  PF_CUDA_TRY(cudaMemsetAsync(cell_start, 0, sizeof(int) * (nc + 1), s));
+  if (n > 0) {
+    k_keys_rank<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, reinterpret_cast<const float4*>(pos4_in), g->dx,
+                                                               g->nx, g->ny, g->nz, key_rank, cell_start);
+    PF_LAUNCHED();
+  }
+  k_scan_tiles<<<(int)tiles, SCAN_NT, 0, s>>>(nc + 1, cell_start, sums);
+  PF_LAUNCHED();
+  k_scan_sums<<<1, SCAN_NT, 0, s>>>((int)tiles, sums);
+  PF_LAUNCHED();
+  k_scan_add<<<grid_for(nc + 1, 256, kNumSMs * 16), 256, 0, s>>>(nc + 1, cell_start, sums, nullptr);
+  PF_LAUNCHED();
+  if (n == 0) return PF_OK;
+  k_scatter_rank<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, key_rank, cell_start, perm_out);
+  PF_LAUNCHED();
+  k_fix_order<<<grid_for(nc * 32, 256, kNumSMs * 16), 256, 0, s>>>((int)nc, cell_start, perm_out, keys_out);
+  PF_LAUNCHED();
+  k_gather<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, perm_out, reinterpret_cast<const float4*>(pos4_in),
+                                                          reinterpret_cast<const float4*>(vel4_in),
+                                                          reinterpret_cast<float4*>(pos4_out),
+                                                          reinterpret_cast<float4*>(vel4_out));
+  PF_LAUNCHED();
+  return PF_OK;
+}

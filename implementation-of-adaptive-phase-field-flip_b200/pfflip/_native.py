@@ -24,6 +24,7 @@ PF_ERR_NOT_CONVERGED = 4
 PF_ERR_WORKSPACE = 5
 PF_ERR_UNSUPPORTED = 6
 
+PF_SORT_STATIC_MAX_CELLS = 512 ** 3
 PF_MG_MAX_LEVELS = 16
 PF_MG_STATE_BYTES = 512
 PF_MG_COUNTERS = 32
@@ -81,6 +82,7 @@ SIGNATURES = {
     "pf_launch_count": (C.c_uint64, []),
     "pf_sort_workspace_bytes": (C.c_size_t, [_G, _I64]),
     "pf_sort_particles": (C.c_int, [_G, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, C.c_size_t, _VP]),
+    "pf_sort_particles_static": (C.c_int, [_G, _I64] + [_VP] * 7 + [_VP]),
     "pf_p2g": (C.c_int, [_G, _I64, _VP, _VP, _VP, _F, _F, _F] + [_VP] * 8 + [_VP]),
     "pf_phase_beta": (C.c_int, [_G] + [_VP] * 7 + [_VP] + [_F] * 6 + [_VP] * 14 + [_VP]),
     "pf_save_and_force": (C.c_int, [_G] + [_VP] * 6 + [_VP, _F, _F, _F, _F, _VP]),

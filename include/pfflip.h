@@ -94,6 +94,23 @@ int pf_sort_particles(const pf_grid* g, int64_t n, const float* pos4_in, const f
                       float* vel4_out, int32_t* keys_out, int32_t* perm_out, int32_t* cell_start, void* workspace,
                       size_t workspace_bytes, void* stream);
 
+/* The same sort without a caller workspace; no counterpart in the reference.
+ * For hosts that cannot hand over device scratch (all device memory fixed at
+ * start-up, or a step that must not allocate).  Arguments, outputs and
+ * results are those of pf_sort_particles.  The call allocates nothing:
+ * per-particle scratch lives in pos4_out until the final gather, and the
+ * scan's tile sums sit in a static device array of the library (131,328
+ * bytes), which limits the grid to PF_SORT_STATIC_MAX_CELLS cells; larger
+ * grids return PF_ERR_ARG.  cell_start is cleared on the stream each call;
+ * nothing else needs to start at zero.  The first call on a device looks up
+ * the array's address (cudaGetSymbolAddress): make it before any stream
+ * capture.  All calls on a device share the array, so calls whose executions
+ * overlap (different streams or host threads) race: order them. */
+#define PF_SORT_STATIC_MAX_CELLS 134217728LL /* 512^3 */
+int pf_sort_particles_static(const pf_grid* g, int64_t n, const float* pos4_in, const float* vel4_in,
+                             float* pos4_out, float* vel4_out, int32_t* keys_out, int32_t* perm_out,
+                             int32_t* cell_start, void* stream);
+
 /* P2G: replaces pfflip/kernels.py:100-158 (p2g_face, x3 axes) and :161-209
  * (p2g_cell) as launched by pfflip/sim.py:205-228, including the zeroing of the
  * 8 accumulators.  Eq. (6) weights with support radius r_p; particle mass is
