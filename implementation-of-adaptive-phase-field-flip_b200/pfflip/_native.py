@@ -102,6 +102,14 @@ SIGNATURES = {
     "pf_mg_precondition": (C.c_int, [_VP, _VP, _VP, _VP]),
     "pf_mg_smooth": (C.c_int, [_VP, _I32, _I32, _I32, _VP]),
     "pf_mg_solve": (C.c_int, [_VP, _VP, _VP, _F, _I32, _I32, _I32, C.POINTER(_I32), C.POINTER(_D), _VP]),
+    "pf_adj_g2p_advect": (C.c_int, [_G, _I64, _VP, _VP] + [_VP] * 9 + [_F, _F, _F, C.POINTER(_F), C.POINTER(_F),
+                                                                       _I32, _I32] + [_VP] * 4 + [_VP] * 9 + [_VP]),
+    "pf_adj_extrapolate": (C.c_int, [_G, _VP, _I32] + [_VP] * 15 + [_VP]),
+    "pf_adj_project": (C.c_int, [_G] + [_VP] * 7 + [_F] + [_VP] * 4 + [_VP]),
+    "pf_adj_face_sources": (C.c_int, [_G] + [_VP] * 11 + [_VP] + [_F] * 7 + [_VP] * 15 + [_VP]),
+    "pf_adj_p2g": (C.c_int, [_G, _I64, _VP, _VP, _F, _F, _F] + [_VP] * 7 + [_VP, _VP, _VP]),
+    "pf_adj_phase_cell": (C.c_int, [_G, _VP, _VP, _F, _F, _F, _VP, _VP]),
+    "pf_adj_unsort": (C.c_int, [_I64, _VP, _VP, _VP, _VP, _VP, _VP]),
 }
 
 

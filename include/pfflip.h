@@ -266,6 +266,85 @@ int pf_mg_smooth(pf_mg_plan* plan, int32_t lv, int32_t nsweeps, int32_t reverse,
 int pf_mg_solve(pf_mg_plan* plan, const float* b, float* x, float tol, int32_t max_iter, int32_t use_graphs,
                 int32_t verbose, int32_t* iters_out, double* rel_out, void* stream);
 
+/* --------------------------------------------------------------- adjoint */
+/* Reverse-mode counterparts of the step's stages.  The reference step
+ * (pfflip/sim.py:168-202) is not differentiable, so none of these replaces a
+ * reference entry point; each is the vector-Jacobian product of the forward
+ * stage cited.  Discrete decisions (sort order, liquid tags, extrapolation
+ * masks, wall clamps, the valid-face test) are held fixed.  Particle
+ * adjoints are float4 streams (x, y, z, unused) in the order of pos4/vel4.
+ * The adjoint of the pressure solve is an MG-PCG solve by the caller:
+ * lam = pf_mg_solve(plan built for the same beta, b = p_bar).  Order of use
+ * for one step, in reverse:
+ *   pf_adj_g2p_advect -> pf_adj_extrapolate -> pf_adj_project -> pf_mg_solve
+ *   -> pf_adj_face_sources -> pf_adj_p2g -> pf_adj_unsort.
+ * Face-grid adjoint outputs marked "accumulate" must be zeroed by the caller. */
+
+/* G2P + Ralston RK3 + wall reflection (pfflip/kernels.py:468-549, :567-595).
+ * pos4/vel4: the particles at the start of the step (sorted order); vel_*:
+ * the projected field u, vstar_*: u*, vliq_*: the extrapolated field.
+ * gpos4_in/gvel4_in: adjoints of the particles after the step.  Writes
+ * gpos4_out/gvel4_out (adjoints at the start of the step, G2P/advection part)
+ * and accumulates into gvel_* (u), gvstar_* (u*) and gvliq_* (extrapolated). */
+int pf_adj_g2p_advect(const pf_grid* g, int64_t n, const float* pos4, const float* vel4, const float* vel_x,
+                      const float* vel_y, const float* vel_z, const float* vstar_x, const float* vstar_y,
+                      const float* vstar_z, const float* vliq_x, const float* vliq_y, const float* vliq_z,
+                      float alpha_liquid, float alpha_air, float dt, const float lo[3], const float hi[3],
+                      int32_t do_g2p, int32_t do_advect, const float* gpos4_in, const float* gvel4_in,
+                      float* gpos4_out, float* gvel4_out, float* gvel_x, float* gvel_y, float* gvel_z,
+                      float* gvstar_x, float* gvstar_y, float* gvstar_z, float* gvliq_x, float* gvliq_y,
+                      float* gvliq_z, void* stream);
+
+/* Transpose of the liquid extrapolation (pfflip/kernels.py:406-462) with
+ * `sweeps` Jacobi sweeps.  gliq_*: adjoint of the extrapolated field (used as
+ * scratch, destroyed); tmp_*: face-sized float scratch; level_*, level_tmp_*:
+ * face-sized byte scratch.  Accumulates into gvel_*. */
+int pf_adj_extrapolate(const pf_grid* g, const int32_t* is_liquid, int32_t sweeps, float* gliq_x, float* gliq_y,
+                       float* gliq_z, float* tmp_x, float* tmp_y, float* tmp_z, uint8_t* level_x, uint8_t* level_y,
+                       uint8_t* level_z, uint8_t* level_tmp_x, uint8_t* level_tmp_y, uint8_t* level_tmp_z,
+                       float* gvel_x, float* gvel_y, float* gvel_z, void* stream);
+
+/* Projection u -= dt*beta*(p_i - p_{i-1})/dx (pfflip/kernels.py:366-387):
+ * writes gp (cells, the right-hand side of the adjoint solve) and gbeta_*
+ * (faces) from the adjoint gvel_* of the projected field. */
+int pf_adj_project(const pf_grid* g, const float* p, const float* beta_x, const float* beta_y, const float* beta_z,
+                   const float* gvel_x, const float* gvel_y, const float* gvel_z, float dt, float* gp,
+                   float* gbeta_x, float* gbeta_y, float* gbeta_z, void* stream);
+
+/* Face sources of the solve, from the adjoint solution lam: the divergence
+ * right-hand side (pfflip/kernels.py:338-363, k_div = 0), gravity and wall
+ * zeroing (:332-335, :314-326), the u* copy (pfflip/sim.py:176-177), eq. (9)
+ * beta with eq. (7) at mixed faces (pfflip/kernels.py:258-311), the
+ * operator's beta sensitivity -(lam_i - lam_j)(p_i - p_j), and u = P/m
+ * (:212-228).  gvel_*: adjoint of u after projection (all contributions),
+ * gvstar_*: adjoint of u*, gbeta_*: from pf_adj_project.  Writes the
+ * adjoints of the P2G face accumulators, gmass_* and gmom_*. */
+int pf_adj_face_sources(const pf_grid* g, const float* p, const float* lam, const float* beta_x, const float* beta_y,
+                        const float* beta_z, const float* mass_x, const float* mass_y, const float* mass_z,
+                        const float* mom_x, const float* mom_y, const float* mom_z, const int32_t* is_liquid,
+                        float mass_eps, float rho_min, float alpha_phi, float rho_0l, float rho_l, float rho_g,
+                        float dt, const float* gvel_x, const float* gvel_y, const float* gvel_z,
+                        const float* gvstar_x, const float* gvstar_y, const float* gvstar_z, const float* gbeta_x,
+                        const float* gbeta_y, const float* gbeta_z, float* gmass_x, float* gmass_y, float* gmass_z,
+                        float* gmom_x, float* gmom_y, float* gmom_z, void* stream);
+
+/* P2G splat, eq. (6) (pfflip/kernels.py:100-209): a per-particle gather of
+ * the face mass/momentum adjoints (all six, or all NULL) and of the cell-mass
+ * adjoint (gcell_mass, may be NULL).  Accumulates into gpos4/gvel4. */
+int pf_adj_p2g(const pf_grid* g, int64_t n, const float* pos4, const float* vel4, float rho_l, float rho_g, float r_p,
+               const float* gmass_x, const float* gmass_y, const float* gmass_z, const float* gmom_x,
+               const float* gmom_y, const float* gmom_z, const float* gcell_mass, float* gpos4, float* gvel4,
+               void* stream);
+
+/* eq. (7) on cells (pfflip/kernels.py:234-255): gcell_mass = dphi/dm * gphi,
+ * zero on the clamped pieces. */
+int pf_adj_phase_cell(const pf_grid* g, const float* cell_mass, const float* gphi, float rho_min, float alpha_phi,
+                      float rho_0l, float* gcell_mass, void* stream);
+
+/* Adjoint of the sort's gather: out[perm[t]] = in[t] for both streams. */
+int pf_adj_unsort(int64_t n, const int32_t* perm, const float* gpos4_sorted, const float* gvel4_sorted,
+                  float* gpos4_out, float* gvel4_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
