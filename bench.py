@@ -70,6 +70,14 @@ def parse():
                     help="comma list of precision_stencil variants for the solve leg")
     ap.add_argument("--solve-repeats", type=int, default=5)
     ap.add_argument("--no-graphs", action="store_true", help="solve leg without CUDA graphs")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-asteroid gradient leg")
+    ap.add_argument("--adjoint-only", action="store_true", help="only the gradient leg (prints its JSON)")
+    ap.add_argument("--adjoint-res", type=int, default=64)
+    ap.add_argument("--adjoint-steps", type=int, default=20)
+    ap.add_argument("--adjoint-fd", action="store_true",
+                    help="check the gradient against FP64 central differences of the CPU oracle (slow)")
+    ap.add_argument("--adjoint-fd-res", type=int, default=None,
+                    help="grid of the finite-difference check (default: --adjoint-res)")
     return ap.parse_args()
 
 
@@ -350,9 +358,15 @@ def run_ours(args):
 
     # mixed-precision step
     if not args.no_mixed and rank == 0 and args.precision == "fp32":
-        del sim
+        sim = None
         torch.cuda.empty_cache()
         line["mixed"] = mixed_leg(args, pos, vel, pt, dt, ms)
+
+    # differentiable asteroid: gradient of |phi_T - phi*|^2 with respect to v0
+    if not args.no_adjoint and rank == 0:
+        sim = None
+        torch.cuda.empty_cache()
+        line["adjoint"] = adjoint_leg(args)
 
     # CPU baseline: the oracle on a bounded sample of the same workload
     if not args.no_cpu_baseline and rank == 0 and world == 1:
@@ -437,10 +451,112 @@ def mixed_leg(args, pos, vel, pt, dt, ms_fp32):
     return res
 
 
+def adjoint_leg(args):
+    """Differentiable asteroid: liquid pool y < 0.3 plus a liquid sphere (r = 0.1
+    at (0.5, 0.7, 0.5)) moving with v0 + N(0, 0.01^2) perturbations, 8 ppc; loss
+    |phi_T - phi*|^2 with phi* from a run with v0 = (0.5, -2, 0); gradient with
+    respect to v0 through the adjoint kernels, checkpoint every 5 steps."""
+    import dataclasses
+
+    import torch
+
+    from pfflip import Config, scenes
+    from pfflip.adjoint import DiffSim
+
+    steps, every = args.adjoint_steps, 5
+
+    def setup(r):
+        cfg = Config(res=(r, r, r), dx=1.0 / r, ppc=8, seed=42, droplets=False, pcg_tol=1e-6, pcg_max_iter=400,
+                     device="cuda")
+        pos, vel, pt, sphere, pert = scenes.asteroid_pool(cfg, v0=(0.0, -2.0, 0.0))
+        base = np.zeros_like(vel)
+        base[sphere] = pert[sphere]
+        return cfg, 0.25 * cfg.dx / 2.5, pos, pt, sphere, base
+
+    def gpu_grad(cfg, dt, pos, pt, sphere, base, timed):
+        ds = DiffSim(cfg, pt, dt, checkpoint_every=every, adjoint_tol=1e-6)
+        dev = torch.device("cuda")
+        x0 = torch.from_numpy(pos).to(dev)
+        b0 = torch.from_numpy(base).to(dev)
+        mask = torch.from_numpy(sphere).to(dev)[:, None].float()
+        with torch.no_grad():
+            vt = b0 + mask * torch.tensor([0.5, -2.0, 0.0], device=dev)[None, :]
+            phi_star = ds.phase_field(ds.rollout(x0, vt, steps)[0]).double()
+
+        def run():
+            v0 = torch.tensor([0.0, -2.0, 0.0], device=dev, requires_grad=True)
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            torch.cuda.synchronize()
+            e0.record()
+            xT, _ = ds.rollout(x0, b0 + mask * v0[None, :], steps)
+            loss = ((ds.phase_field(xT).double() - phi_star) ** 2).sum()
+            e1.record()
+            loss.backward()
+            e2.record()
+            torch.cuda.synchronize()
+            return float(loss.detach()), v0.grad.double().cpu().numpy(), e0.elapsed_time(e1), e1.elapsed_time(e2)
+
+        if timed:
+            run()  # warm-up
+        ds.adjoint_solves.clear()
+        out = run()
+        solves = list(ds.adjoint_solves)
+        phs = phi_star.cpu().numpy()
+        del ds
+        torch.cuda.empty_cache()
+        return out, solves, phs
+
+    r = args.adjoint_res
+    cfg, dt, pos, pt, sphere, base = setup(r)
+    (loss, grad, fwd_ms, bwd_ms), solves, phs = gpu_grad(cfg, dt, pos, pt, sphere, base, True)
+    out = {"workload": f"differentiable asteroid {r}^3 8ppc, {steps} steps, checkpoint every {every}",
+           "particles": int(len(pos)), "dt": dt, "loss": loss, "grad_v0": grad.tolist(),
+           "forward_ms": fwd_ms, "backward_ms": bwd_ms, "forward_ms_per_step": fwd_ms / steps,
+           "backward_ms_per_step": bwd_ms / steps,
+           "adjoint_solve_iters_mean": float(np.mean([it for it, _ in solves])),
+           "adjoint_solve_rel_max": float(max(rel for _, rel in solves))}
+    if args.adjoint_fd:
+        from oracle import oracle as O
+
+        fr = args.adjoint_fd_res or r
+        if fr != r:
+            cfg, dt, pos, pt, sphere, base = setup(fr)
+            (_, grad, _, _), _, phs = gpu_grad(cfg, dt, pos, pt, sphere, base, False)
+        threads = os.cpu_count() or 1
+        c64 = dataclasses.replace(cfg, pcg_tol=1e-12, pcg_max_iter=1000)
+
+        def fd_loss(v):
+            vv = base.astype(np.float64)
+            vv[sphere] += v
+            sim = O.OracleSim(c64, dtype=np.float64, nthreads=threads, stencil="flux")
+            sim.set_particles(pos, vv, pt)
+            for _ in range(steps):
+                sim.step(dt)
+            sim._p2g()
+            sim._phase_field_and_coefficients()
+            return float(((sim.phi_cell - phs) ** 2).sum())
+
+        eps = 1e-6
+        v = np.array([0.0, -2.0, 0.0])
+        t0 = time.perf_counter()
+        fd = np.array([(fd_loss(v + eps * e) - fd_loss(v - eps * e)) / (2 * eps) for e in np.eye(3)])
+        out["fd_check"] = {"res": fr, "grad_v0": grad.tolist(), "fd_grad_v0": fd.tolist(), "eps": eps,
+                           "oracle": "binary64, solve to 1e-12",
+                           "max_rel_err": float(np.abs(grad - fd).max() / np.abs(fd).max()),
+                           "cpu_s": time.perf_counter() - t0, "threads": threads}
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.adjoint_only:
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps({"adjoint": adjoint_leg(args)}), flush=True)
+        return 0
     if args.solve_only:
         import torch
 
