@@ -12,7 +12,7 @@
 // for power-of-two dx, within an ulp otherwise.
 // Particles are in cell order, so neighbouring threads gather neighbouring
 // taps from L1/L2.
-#include "pf_common.cuh"
+#include "pf_faces.cuh"
 
 namespace pf {
 
@@ -93,6 +93,39 @@ __device__ __forceinline__ void sample_vel(const float* const f[3], const float 
   for (int c = 0; c < 3; ++c) out[c] = sample_c<false>(f[c], nullptr, c, fr, ny, nz);
 }
 
+// pfflip/kernels.py:630-679: a particle inside a solid cell moves out along the
+// axis with the nearest free cell (at most 7 cells), its inward velocity zeroed
+__device__ __forceinline__ void push_out_of_solids(const int* __restrict__ solid, int nx, int ny, int nz, float dx,
+                                                   float x[3], float v[3]) {
+  const int i = min(max((int)(x[0] / dx), 0), nx - 1);
+  const int j = min(max((int)(x[1] / dx), 0), ny - 1);
+  const int k = min(max((int)(x[2] / dx), 0), nz - 1);
+  if (solid[((long long)i * ny + j) * nz + k] == 0) return;
+  float best = 1.0e9f;
+  int bax = 0, bsg = 1;
+  for (int d = 0; d < 6; ++d) {
+    const int ax = d / 2, sg = (d % 2 == 0) ? -1 : 1;
+    for (int t = 1; t < 8; ++t) {
+      const int ii = i + (ax == 0 ? sg * t : 0), jj = j + (ax == 1 ? sg * t : 0), kk = k + (ax == 2 ? sg * t : 0);
+      if (ii < 0 || jj < 0 || kk < 0 || ii >= nx || jj >= ny || kk >= nz) break;
+      if (solid[((long long)ii * ny + jj) * nz + kk] == 0) {
+        const float dist = (float)t;
+        if (dist < best) {
+          best = dist;
+          bax = ax;
+          bsg = sg;
+        }
+        break;
+      }
+    }
+  }
+  if (best <= 1.0e8f) {
+    const float off = (best + 0.5f) * dx * (float)bsg;
+    x[bax] = x[bax] + off;
+    if ((float)bsg * v[bax] < 0.f) v[bax] = 0.f;
+  }
+}
+
 __global__ void __launch_bounds__(256) k_g2p_advect(G2PArgs a) {
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
     float4 P = a.pos[p];
@@ -143,38 +176,193 @@ __global__ void __launch_bounds__(256) k_g2p_advect(G2PArgs a) {
             v[c] = fminf(v[c], 0.f);
           }
         }
-        if (a.solid) {  // pfflip/kernels.py:630-679
-          const int nx = a.nx, ny = a.ny, nz = a.nz;
-          const int i = min(max((int)(x[0] / a.dx), 0), nx - 1);
-          const int j = min(max((int)(x[1] / a.dx), 0), ny - 1);
-          const int k = min(max((int)(x[2] / a.dx), 0), nz - 1);
-          if (a.solid[((long long)i * ny + j) * nz + k] != 0) {
-            float best = 1.0e9f;
-            int bax = 0, bsg = 1;
-            for (int d = 0; d < 6; ++d) {
-              const int ax = d / 2, sg = (d % 2 == 0) ? -1 : 1;
-              for (int t = 1; t < 8; ++t) {
-                const int ii = i + (ax == 0 ? sg * t : 0), jj = j + (ax == 1 ? sg * t : 0),
-                          kk = k + (ax == 2 ? sg * t : 0);
-                if (ii < 0 || jj < 0 || kk < 0 || ii >= nx || jj >= ny || kk >= nz) break;
-                if (a.solid[((long long)ii * ny + jj) * nz + kk] == 0) {
-                  const float dist = (float)t;
-                  if (dist < best) {
-                    best = dist;
-                    bax = ax;
-                    bsg = sg;
-                  }
-                  break;
-                }
-              }
-            }
-            if (best <= 1.0e8f) {
-              const float off = (best + 0.5f) * a.dx * (float)bsg;
-              x[bax] = x[bax] + off;
-              if ((float)bsg * v[bax] < 0.f) v[bax] = 0.f;
-            }
+        if (a.solid) push_out_of_solids(a.solid, a.nx, a.ny, a.nz, a.dx, x, v);
+      }
+    }
+    P.x = x[0]; P.y = x[1]; P.z = x[2];
+    V.x = v[0]; V.y = v[1]; V.z = v[2];
+    a.pos[p] = P;
+    a.vel[p] = V;
+  }
+}
+
+// ---------------------------------------------------------------- paired taps
+// The same particle pass reading the face fields through k-paired copies:
+// uu[c][f] = (u[f], u[f+1], u*[f], u*[f+1]) and ul[c][f] = (ul[f], ul[f+1])
+// along k (f+1 -> f on the last k plane).  A trilinear sample then needs four
+// row loads (one per (i, j) tap pair) instead of eight gathers, and G2P reads u
+// and u* with one 16-byte load per row.  Where the frame clamps the k taps to
+// one index (lo == hi) the upper tap takes the lower value, so every tap value
+// and every sum is the one the unpaired kernel forms.
+struct FacePack {
+  FaceSpace s;
+  const float* u[3];
+  const float* us[3];
+  const float* ul[3];
+  float4* uu[3];
+  float2* ul2[3];
+};
+
+struct G2PPackedArgs {
+  long long n;
+  int nx, ny, nz;
+  float dx, inv_dx, dt, a_liq, a_air;
+  float lo[3], hi[3];
+  float4* pos;
+  float4* vel;
+  const float4* uu[3];
+  const float2* ul[3];
+  const int* solid;
+  int do_g2p, do_advect;
+};
+
+__global__ void __launch_bounds__(C3_NT) k_pack_faces(FacePack fp) {
+  long long f;
+  int i, j, k;
+  const int ax = locate(fp.s, &f, &i, &j, &k);
+  if (ax < 0 || ax > 2) return;
+  const int n2 = fp.s.nz + (ax == 2);
+  const long long fn = (k < n2 - 1) ? f + 1 : f;
+  const float* u = fp.u[ax];
+  const float* us = fp.us[ax];
+  fp.uu[ax][f] = make_float4(u[f], u[fn], us ? us[f] : 0.f, us ? us[fn] : 0.f);
+  if (fp.ul2[ax]) fp.ul2[ax][f] = make_float2(fp.ul[ax][f], fp.ul[ax][fn]);
+}
+
+// (di, dj) row offsets and k-tap selection of face grid c for a frame
+struct Rows {
+  int row[4];
+  float wij[4];
+  float wk0, wk1;
+  bool clampk;
+};
+
+__device__ __forceinline__ void rows_of(const Frame& fr, int c, int ny, int nz, Rows& r) {
+  const int vi = c == 0 ? 0 : 1, vj = c == 1 ? 0 : 1, vk = c == 2 ? 0 : 1;
+  const int n1 = ny + (c == 1), n2 = nz + (c == 2);
+  const float tx = fr.t[0][vi], ty = fr.t[1][vj], tz = fr.t[2][vk];
+  const int I[2] = {fr.lo[0][vi], fr.hi[0][vi]}, J[2] = {fr.lo[1][vj], fr.hi[1][vj]};
+  const float wi[2] = {1.f - tx, tx}, wj[2] = {1.f - ty, ty};
+#pragma unroll
+  for (int di = 0; di < 2; ++di)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj) {
+      r.row[di * 2 + dj] = (I[di] * n1 + J[dj]) * n2 + fr.lo[2][vk];
+      r.wij[di * 2 + dj] = wi[di] * wj[dj];
+    }
+  r.wk0 = 1.f - tz;
+  r.wk1 = tz;
+  r.clampk = fr.lo[2][vk] == fr.hi[2][vk];
+}
+
+// G2P sample of component c: delta = I(u - u*) tap by tap, pic = I(u)
+__device__ __forceinline__ void sample_g2p_packed(const float4* __restrict__ uu, const Rows& r, float& delta,
+                                                  float& pic) {
+  float ad = 0.f, ap = 0.f;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float4 v = __ldg(uu + r.row[q]);
+    const float u1 = r.clampk ? v.x : v.y, s1 = r.clampk ? v.z : v.w;
+    ad += r.wij[q] * r.wk0 * (v.x - v.z);
+    ad += r.wij[q] * r.wk1 * (u1 - s1);
+    ap += r.wij[q] * r.wk0 * v.x;
+    ap += r.wij[q] * r.wk1 * u1;
+  }
+  delta = ad;
+  pic = ap;
+}
+
+__device__ __forceinline__ float sample_pair2(const float2* __restrict__ f, const Rows& r) {
+  float acc = 0.f;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float2 v = __ldg(f + r.row[q]);
+    const float h = r.clampk ? v.x : v.y;
+    acc += r.wij[q] * r.wk0 * v.x;
+    acc += r.wij[q] * r.wk1 * h;
+  }
+  return acc;
+}
+
+__device__ __forceinline__ float sample_pair4(const float4* __restrict__ f, const Rows& r) {
+  float acc = 0.f;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float4 v = __ldg(f + r.row[q]);
+    const float h = r.clampk ? v.x : v.y;
+    acc += r.wij[q] * r.wk0 * v.x;
+    acc += r.wij[q] * r.wk1 * h;
+  }
+  return acc;
+}
+
+// RK3 sample: liquid particles read the extrapolated field, air the raw one
+__device__ __forceinline__ void sample_vel_packed(const G2PPackedArgs& a, bool liquid, const Frame& fr,
+                                                  float out[3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    Rows r;
+    rows_of(fr, c, a.ny, a.nz, r);
+    out[c] = liquid ? sample_pair2(a.ul[c], r) : sample_pair4(a.uu[c], r);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_g2p_advect_packed(G2PPackedArgs a) {
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
+    float4 P = a.pos[p];
+    float4 V = a.vel[p];
+    const int flags = __float_as_int(P.w);
+    const int pstate = (flags >> PF_PSTATE_SHIFT) & 3;
+    const bool liquid = (flags & PF_FLAG_LIQUID) != 0;
+    float x[3] = {P.x, P.y, P.z};
+    float v[3] = {V.x, V.y, V.z};
+    const bool flip = pstate == 0;
+    Frame fx;
+    if (flip && (a.do_g2p || a.do_advect)) make_frame(x, a.inv_dx, a.nx, a.ny, a.nz, fx);
+    if (a.do_g2p && flip) {
+      const float alpha = liquid ? a.a_liq : a.a_air;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        Rows r;
+        rows_of(fx, c, a.ny, a.nz, r);
+        float delta, pic;
+        sample_g2p_packed(a.uu[c], r, delta, pic);
+        v[c] = alpha * (v[c] + delta) + (1.f - alpha) * pic;
+      }
+    }
+    if (a.do_advect) {
+      if (flip) {
+        float k1[3], k2[3], k3[3], y[3];
+        sample_vel_packed(a, liquid, fx, k1);
+        const float h1 = 0.5f * a.dt, h2 = 0.75f * a.dt;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) y[c] = x[c] + h1 * k1[c];
+        Frame fy;
+        make_frame(y, a.inv_dx, a.nx, a.ny, a.nz, fy);
+        sample_vel_packed(a, liquid, fy, k2);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) y[c] = x[c] + h2 * k2[c];
+        make_frame(y, a.inv_dx, a.nx, a.ny, a.nz, fy);
+        sample_vel_packed(a, liquid, fy, k3);
+        const float c1 = 2.0f / 9.0f, c2 = 3.0f / 9.0f, c3 = 4.0f / 9.0f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float xn = x[c] + a.dt * (c1 * k1[c] + c2 * k2[c] + c3 * k3[c]);
+          x[c] = fminf(fmaxf(xn, a.lo[c]), a.hi[c]);
+        }
+      }
+      if (pstate != 2) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (x[c] <= a.lo[c]) {
+            x[c] = a.lo[c];
+            v[c] = fmaxf(v[c], 0.f);
+          } else if (x[c] >= a.hi[c]) {
+            x[c] = a.hi[c];
+            v[c] = fminf(v[c], 0.f);
           }
         }
+        if (a.solid) push_out_of_solids(a.solid, a.nx, a.ny, a.nz, a.dx, x, v);
       }
     }
     P.x = x[0]; P.y = x[1]; P.z = x[2];
@@ -218,6 +406,92 @@ extern "C" int pf_g2p_advect(const pf_grid* g, int64_t n, float* pos4, float* ve
   a.do_g2p = do_g2p;
   a.do_advect = do_advect;
   k_g2p_advect<<<grid_for(n, 256, kNumSMs * 16), 256, 0, S(stream)>>>(a);
+  PF_LAUNCHED();
+  return PF_OK;
+}
+
+namespace {
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// workspace layout: per axis the float4 (u, u*) pairs, then the float2 ul pairs
+size_t packed_bytes(const pf_grid* g, size_t offs[6]) {
+  const FaceSpace sp = make_space(g->nx, g->ny, g->nz);
+  size_t off = 0;
+  for (int c = 0; c < 3; ++c) {
+    offs[c] = off;
+    off += align256((size_t)sp.nf[c] * sizeof(float4));
+  }
+  for (int c = 0; c < 3; ++c) {
+    offs[3 + c] = off;
+    off += align256((size_t)sp.nf[c] * sizeof(float2));
+  }
+  return off;
+}
+
+}  // namespace
+
+extern "C" size_t pf_g2p_workspace_bytes(const pf_grid* g) {
+  if (!g || g->nx <= 0 || g->ny <= 0 || g->nz <= 0) return 0;
+  size_t offs[6];
+  return packed_bytes(g, offs);
+}
+
+extern "C" int pf_g2p_advect_packed(const pf_grid* g, int64_t n, float* pos4, float* vel4, const float* vel_x,
+                                    const float* vel_y, const float* vel_z, const float* vstar_x,
+                                    const float* vstar_y, const float* vstar_z, const float* vliq_x,
+                                    const float* vliq_y, const float* vliq_z, const int32_t* solid,
+                                    float alpha_liquid, float alpha_air, float dt, const float lo[3],
+                                    const float hi[3], int32_t do_g2p, int32_t do_advect, void* workspace,
+                                    size_t workspace_bytes, void* stream) {
+  PF_REQUIRE(g && pos4 && vel4 && vel_x && vel_y && vel_z, "null argument");
+  PF_REQUIRE(g->nx > 0 && g->ny > 0 && g->nz > 0, "bad grid");
+  PF_REQUIRE(!do_g2p || (vstar_x && vstar_y && vstar_z), "u* fields required for G2P");
+  PF_REQUIRE(!do_advect || (vliq_x && vliq_y && vliq_z && lo && hi), "extrapolated fields and bounds required");
+  PF_REQUIRE(aligned16(pos4) && aligned16(vel4), "particle streams must be 16-byte aligned");
+  size_t offs[6];
+  PF_REQUIRE(workspace && workspace_bytes >= packed_bytes(g, offs), "workspace too small");
+  PF_REQUIRE((reinterpret_cast<uintptr_t>(workspace) & 255) == 0, "workspace must be 256-byte aligned");
+  PF_REQUIRE((long long)g->nx * g->ny * (g->nz + 1) < (1LL << 31) &&
+                 (long long)(g->nx + 1) * g->ny * g->nz < (1LL << 31) &&
+                 (long long)g->nx * (g->ny + 1) * g->nz < (1LL << 31),
+             "face arrays must hold < 2^31 entries");
+  if (n <= 0) return PF_OK;
+  cudaStream_t s = S(stream);
+  unsigned char* ws = static_cast<unsigned char*>(workspace);
+  FacePack fp;
+  fp.s = make_space(g->nx, g->ny, g->nz);
+  const float* u[3] = {vel_x, vel_y, vel_z};
+  const float* us[3] = {vstar_x, vstar_y, vstar_z};
+  const float* ul[3] = {vliq_x, vliq_y, vliq_z};
+  G2PPackedArgs a;
+  for (int c = 0; c < 3; ++c) {
+    fp.u[c] = u[c];
+    fp.us[c] = do_g2p ? us[c] : nullptr;
+    fp.ul[c] = do_advect ? ul[c] : nullptr;
+    fp.uu[c] = reinterpret_cast<float4*>(ws + offs[c]);
+    fp.ul2[c] = do_advect ? reinterpret_cast<float2*>(ws + offs[3 + c]) : nullptr;
+    a.uu[c] = fp.uu[c];
+    a.ul[c] = fp.ul2[c];
+  }
+  k_pack_faces<<<grid_faces(g->nx, g->ny, g->nz, false), C3_NT, 0, s>>>(fp);
+  PF_LAUNCHED();
+  a.n = n;
+  a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
+  a.dx = g->dx;
+  a.inv_dx = (float)(1.0 / (double)g->dx);
+  a.dt = dt;
+  a.a_liq = alpha_liquid; a.a_air = alpha_air;
+  for (int c = 0; c < 3; ++c) {
+    a.lo[c] = lo ? lo[c] : 0.f;
+    a.hi[c] = hi ? hi[c] : 0.f;
+  }
+  a.pos = reinterpret_cast<float4*>(pos4);
+  a.vel = reinterpret_cast<float4*>(vel4);
+  a.solid = solid;
+  a.do_g2p = do_g2p;
+  a.do_advect = do_advect;
+  k_g2p_advect_packed<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(a);
   PF_LAUNCHED();
   return PF_OK;
 }

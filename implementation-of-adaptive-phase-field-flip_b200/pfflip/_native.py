@@ -92,6 +92,10 @@ SIGNATURES = {
     "pf_extrapolate": (C.c_int, [_G, _VP, _VP, _VP, _VP, _I32, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "pf_g2p_advect": (C.c_int, [_G, _I64, _VP, _VP] + [_VP] * 9 + [_VP, _F, _F, _F, C.POINTER(_F),
                                                                      C.POINTER(_F), _I32, _I32, _VP]),
+    "pf_g2p_workspace_bytes": (C.c_size_t, [_G]),
+    "pf_g2p_advect_packed": (C.c_int, [_G, _I64, _VP, _VP] + [_VP] * 9 + [_VP, _F, _F, _F, C.POINTER(_F),
+                                                                          C.POINTER(_F), _I32, _I32, _VP,
+                                                                          C.c_size_t, _VP]),
     "pf_particle_max_speed": (C.c_int, [_I64, _VP, _VP, _VP, _VP]),
     "pf_apply_A": (C.c_int, [_G, _VP, _VP, _VP, _VP, _VP, _VP, _I32, _VP]),
     "pf_mg_partials_count": (C.c_int64, []),

@@ -173,6 +173,7 @@ class Simulator:
         self.stats: list[dict] = []
         self._warned_droplets = False
         self._marks = None  # per-stage CUDA events when stage timing is on
+        self._g2p_ws = None  # k-paired face fields of the G2P/advection pass
 
         self.px = ParticleField(self, "pos")
         self.pv = ParticleField(self, "vel")
@@ -398,10 +399,14 @@ class Simulator:
     def _g2p_advect(self, dt, do_g2p, do_advect):
         lo, hi = self._bounds()
         cfg = self.cfg
-        N.call("pf_g2p_advect", C.byref(self._g), self.n_particles, self._pos4.data_ptr(), self._vel4.data_ptr(),
-               *(N.ptr(a) for a in self.vel), *(N.ptr(a) for a in self.vel_star), *(N.ptr(a) for a in self.vel_liq),
-               N.ptr(self.solid) if self.has_solids else None, float(cfg.alpha_flip_liquid),
-               float(cfg.alpha_flip_air), float(dt), lo, hi, int(do_g2p), int(do_advect), N.stream())
+        if self._g2p_ws is None:
+            nb = int(N.lib().pf_g2p_workspace_bytes(C.byref(self._g)))
+            self._g2p_ws = torch.empty(nb, dtype=torch.uint8, device=self.dev)
+        N.call("pf_g2p_advect_packed", C.byref(self._g), self.n_particles, self._pos4.data_ptr(),
+               self._vel4.data_ptr(), *(N.ptr(a) for a in self.vel), *(N.ptr(a) for a in self.vel_star),
+               *(N.ptr(a) for a in self.vel_liq), N.ptr(self.solid) if self.has_solids else None,
+               float(cfg.alpha_flip_liquid), float(cfg.alpha_flip_air), float(dt), lo, hi, int(do_g2p),
+               int(do_advect), self._g2p_ws.data_ptr(), self._g2p_ws.numel(), N.stream())
 
     def _g2p(self):
         """eq. (11)-(12) FLIP/PIC update (pfflip/sim.py:316-327)."""

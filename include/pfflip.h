@@ -184,6 +184,19 @@ int pf_g2p_advect(const pf_grid* g, int64_t n, float* pos4, float* vel4, const f
                   float alpha_liquid, float alpha_air, float dt, const float lo[3], const float hi[3],
                   int32_t do_g2p, int32_t do_advect, void* stream);
 
+/* The same pass reading the face fields through k-paired copies built in the
+ * caller's workspace (pf_g2p_workspace_bytes, 256-byte aligned): per face,
+ * (u[k], u[k+1], u*[k], u*[k+1]) and (vel_liq[k], vel_liq[k+1]).  A sample
+ * then takes four row loads instead of eight gathers; every tap value and sum
+ * is the one pf_g2p_advect forms.  Same arguments and results otherwise. */
+size_t pf_g2p_workspace_bytes(const pf_grid* g);
+int pf_g2p_advect_packed(const pf_grid* g, int64_t n, float* pos4, float* vel4, const float* vel_x,
+                         const float* vel_y, const float* vel_z, const float* vstar_x, const float* vstar_y,
+                         const float* vstar_z, const float* vliq_x, const float* vliq_y, const float* vliq_z,
+                         const int32_t* solid, float alpha_liquid, float alpha_air, float dt, const float lo[3],
+                         const float hi[3], int32_t do_g2p, int32_t do_advect, void* workspace,
+                         size_t workspace_bytes, void* stream);
+
 /* max |v| over particles with pstate == 0, written to the device float *out;
  * replaces pfflip/kernels.py:552-564 (particle_max_speed). */
 int pf_particle_max_speed(int64_t n, const float* pos4, const float* vel4, float* out, void* stream);

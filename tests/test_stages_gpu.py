@@ -268,3 +268,46 @@ def test_step_matches_oracle_dam_break_32():
     assert np.abs(sim.px.numpy() - o.px).max() < 1e-4 * cfg.dx
     assert rel(sim.pv.numpy(), o.pv) < 1e-3
     assert rel(sim.phi_cell.numpy(), o.phi_cell) < 1e-4
+
+
+@pytest.mark.parametrize("flags", [(1, 1), (1, 0), (0, 1)])
+def test_g2p_packed_matches_unpaired(flags):
+    """pf_g2p_advect_packed reads k-paired copies of the fields; every tap and
+    sum is the unpaired kernel's, so results agree to rounding (FMA contraction
+    may differ): 4 ulps of the largest value."""
+    do_g2p, do_adv = flags
+    res = (24, 20, 36)
+    dx = np.float32(1 / 24)
+    g = N.grid(res, dx)
+    rng = np.random.default_rng(21)
+    n = 100_000
+    L = np.array(res) * float(dx)
+    pos = (rng.random((n, 3)) * L).astype(np.float32)
+    pos[:2000] = (rng.random((2000, 3)) * 1e-3).astype(np.float32)  # at the low walls: clamped taps
+    pos[2000:4000] = (L - rng.random((2000, 3)) * 1e-3).astype(np.float32)  # at the high walls
+    fs = ((25, 20, 36), (24, 21, 36), (24, 20, 37))
+    f = lambda: [torch.tensor(rng.standard_normal(s).astype(np.float32), device=DEV) for s in fs]  # noqa: E731
+    u, us, ul = f(), f(), f()
+    p4 = torch.zeros((n, 4), device=DEV)
+    p4[:, :3] = torch.tensor(pos, device=DEV)
+    p4.view(torch.int32)[:, 3] = torch.tensor((rng.random(n) < 0.5).astype(np.int32), device=DEV)
+    v4 = torch.zeros((n, 4), device=DEV)
+    v4[:, :3] = torch.tensor(rng.standard_normal((n, 3)).astype(np.float32), device=DEV)
+    eps = 1e-4 * float(dx)
+    lo = (C.c_float * 3)(eps, eps, eps)
+    hi = (C.c_float * 3)(*[float(x) - eps for x in L])
+    ws = torch.empty(int(N.lib().pf_g2p_workspace_bytes(C.byref(g))), dtype=torch.uint8, device=DEV)
+    outs = []
+    for packed in (False, True):
+        p, v = p4.clone(), v4.clone()
+        args = [C.byref(g), n, p.data_ptr(), v.data_ptr(), *(t.data_ptr() for t in u), *(t.data_ptr() for t in us),
+                *(t.data_ptr() for t in ul), None, 0.985, 0.96, 0.01, lo, hi, do_g2p, do_adv]
+        if packed:
+            N.call("pf_g2p_advect_packed", *args, ws.data_ptr(), ws.numel(), N.stream())
+        else:
+            N.call("pf_g2p_advect", *args, N.stream())
+        outs.append((p.cpu().numpy(), v.cpu().numpy()))
+    (pa, va), (pb, vb) = outs
+    assert np.array_equal(pa[:, 3].view(np.int32), pb[:, 3].view(np.int32))
+    assert np.abs(pa[:, :3] - pb[:, :3]).max() <= 4 * np.spacing(np.float32(np.abs(pa[:, :3]).max()))
+    assert np.abs(va[:, :3] - vb[:, :3]).max() <= 4 * np.spacing(np.float32(np.abs(va[:, :3]).max()))
