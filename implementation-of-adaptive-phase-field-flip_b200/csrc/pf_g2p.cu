@@ -307,7 +307,7 @@ __device__ __forceinline__ void sample_vel_packed(const G2PPackedArgs& a, bool l
   }
 }
 
-__global__ void __launch_bounds__(256) k_g2p_advect_packed(G2PPackedArgs a) {
+__global__ void __launch_bounds__(256, 4) k_g2p_advect_packed(G2PPackedArgs a) {
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
     float4 P = a.pos[p];
     float4 V = a.vel[p];

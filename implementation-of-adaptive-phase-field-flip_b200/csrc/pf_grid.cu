@@ -252,6 +252,71 @@ __global__ void __launch_bounds__(EX_NT) k_extrapolate(int nx, int ny, int nz, i
   }
 }
 
+// ---------------------------------------------------------------- extrapolation by levels
+// The same extrapolation, computed level by level in place.  A face becomes
+// known at sweep s exactly when it was unknown and has a neighbour known
+// after sweep s-1; from then on every sweep copies it.  So its final value is
+// the mean, over its neighbours of level <= s-1, of their final values, and
+// the faces set in pass s read only faces set in earlier passes.  The known
+// arrays hold the level during the passes (kExNever = not reached) and 0/1
+// at the end.  Sums run over the neighbours in the reference's order (-i, +i,
+// -j, +j, -k, +k), so every value is the reference's.
+constexpr int kExNever = 0x7fffffff;
+
+struct ExLevelArgs {
+  FaceSpace s;
+  const float* vel[3];
+  const int* is_liq;
+  float* out[3];
+  int* lv[3];
+  int pass;  // 0: seed; 1..S: sweep; -1: levels -> 0/1 (S in `last`)
+  int last;
+};
+
+__global__ void __launch_bounds__(C3_NT) k_ex_levels(ExLevelArgs a) {
+  long long f;
+  int i, j, k;
+  const int ax = locate(a.s, &f, &i, &j, &k);
+  if (ax < 0 || ax > 2) return;
+  int* lv = a.lv[ax];
+  if (a.pass == 0) {  // seed_liquid_velocity, pfflip/kernels.py:406-425
+    const int nx = a.s.nx, ny = a.s.ny, nz = a.s.nz;
+    const int im = i - (ax == 0), jm = j - (ax == 1), km = k - (ax == 2);
+    int liq = 0;
+    if (i < nx && j < ny && k < nz) liq = max(liq, a.is_liq[((long long)i * ny + j) * nz + k]);
+    if (im >= 0 && jm >= 0 && km >= 0) liq = max(liq, a.is_liq[((long long)im * ny + jm) * nz + km]);
+    lv[f] = liq == 1 ? 0 : kExNever;
+    a.out[ax][f] = liq == 1 ? a.vel[ax][f] : 0.f;
+    return;
+  }
+  if (a.pass < 0) {
+    lv[f] = lv[f] <= a.last ? 1 : 0;
+    return;
+  }
+  if (lv[f] != kExNever) return;
+  const int n0 = a.s.nx + (ax == 0), n1 = a.s.ny + (ax == 1), n2 = a.s.nz + (ax == 2);
+  const long long st[3] = {(long long)n1 * n2, n2, 1};
+  const int id[3] = {i, j, k}, nn[3] = {n0, n1, n2};
+  const float* out = a.out[ax];
+  float acc = 0.f;
+  int cnt = 0;
+#pragma unroll
+  for (int d = 0; d < 6; ++d) {  // extrapolate_sweep, pfflip/kernels.py:428-462
+    const int ad = d >> 1, sg = (d & 1) ? 1 : -1;
+    const int q = id[ad] + sg;
+    if (q < 0 || q >= nn[ad]) continue;
+    const long long g = f + sg * st[ad];
+    if (lv[g] <= a.pass - 1) {
+      acc += out[g];
+      cnt += 1;
+    }
+  }
+  if (cnt > 0) {
+    a.out[ax][f] = acc / (float)cnt;
+    lv[f] = a.pass;
+  }
+}
+
 // CFL speed over particles with pstate == 0 (pfflip/kernels.py:552-564)
 __global__ void __launch_bounds__(256) k_max_speed(long long n, const float4* __restrict__ pos,
                                                    const float4* __restrict__ vel, float* out) {
@@ -365,6 +430,24 @@ int pf_extrapolate(const pf_grid* g, const float* vel_x, const float* vel_y, con
   const float* vin[3] = {vel_x, vel_y, vel_z};
   float* vout[3] = {vel_liq_x, vel_liq_y, vel_liq_z};
   int* kout[3] = {known_x, known_y, known_z};
+  if (known_x && known_y && known_z) {  // level passes, in place in vel_liq and known
+    ExLevelArgs a;
+    a.s = make_space(g->nx, g->ny, g->nz);
+    for (int c = 0; c < 3; ++c) {
+      a.vel[c] = vin[c];
+      a.out[c] = vout[c];
+      a.lv[c] = kout[c];
+    }
+    a.is_liq = is_liquid;
+    a.last = sweeps;
+    const dim3 grid = grid_faces(g->nx, g->ny, g->nz, false);
+    for (int pass = 0; pass <= sweeps + 1; ++pass) {
+      a.pass = pass <= sweeps ? pass : -1;
+      k_ex_levels<<<grid, C3_NT, 0, S(stream)>>>(a);
+      PF_LAUNCHED();
+    }
+    return PF_OK;
+  }
   const int H = sweeps;
   const size_t rn = (size_t)(EX_TI + 2 * H) * (EX_TJ + 2 * H) * (EX_TK + 2 * H);
   const size_t smem = rn * (2 * sizeof(float) + 2);

@@ -699,6 +699,7 @@ template <class T, class TB> struct BottomArgs {
   int flux;
   MGState* st;
   int want_mean, mixed;
+  int bulk;  // stage faces and b with cp.async.bulk (fp32 storage, 16-byte sizes)
 };
 
 __host__ __device__ inline size_t bottom_level_floats(int n0, int n1, int n2) {
@@ -753,6 +754,94 @@ __device__ __forceinline__ void bt_relax(R* P, const float* B, const float* X, c
     res = (R)B[e] - (d * pv - sum);
   }
   P[e] = pv + omega * res / d;
+}
+
+// `sweeps` red-black sweeps of a coarsest level of at most 64 cells with an
+// even k extent, by one warp with everything in registers.  Lane l holds the
+// cells 2l and 2l+1 (same row, k = 2h and 2h+1): one of each colour.  For a
+// half-sweep of colour c every lane publishes its other-colour cell; that is
+// exactly the value each neighbour of a colour-c cell needs (its +-i and +-j
+// neighbours sit at the same k in lanes l -+ n1*n2/2 and l -+ n2/2, its +-k
+// neighbours are the lane's own other cell or the one published by lane l-+1).
+// Neighbours past the walls take the cell's own value, as bt_relax clamps
+// them.  Faces, b and the diagonal are read once; the row arithmetic is
+// bt_relax's, operation for operation, so the result equals the shared-memory
+// sweeps bit for bit.  P (AccT, shared) holds zeros on entry and the solution
+// on return.
+template <class R>
+__device__ __forceinline__ void bt_coarsest_regs(const BottomLevel& L, R* P, const float* B, const float* X,
+                                                 const float* Y, const float* Z, R omega, int sweeps, int flux,
+                                                 int lane) {
+  const int n0 = L.n0, n1 = L.n1, n2 = L.n2, hk = n2 >> 1;
+  const int half = (n0 * n1 * n2) >> 1;
+  const bool act = lane < half;
+  const int l = act ? lane : 0;
+  const int h = l % hk, row = l / hk, j = row % n1, i = row / n1;
+  const int sI = n1 * n2;
+  float cx0[2], cx1[2], cy0[2], cy1[2], cz0[2], cz1[2], cb[2], cd[2];  // as stored; widened at use
+  R p[2];
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const int k = 2 * h + s, e = (i * n1 + j) * n2 + k;
+    const int fyi = (i * (n1 + 1) + j) * n2 + k, fzi = (i * n1 + j) * (n2 + 1) + k;
+    cx0[s] = X[e];
+    cx1[s] = X[e + sI];
+    cy0[s] = Y[fyi];
+    cy1[s] = Y[fyi + n2];
+    cz0[s] = Z[fzi];
+    cz1[s] = Z[fzi + 1];
+    cd[s] = X[e] + X[e + sI] + Y[fyi] + Y[fyi + n2] + Z[fzi] + Z[fzi + 1];
+    cb[s] = B[e];
+    p[s] = act ? P[2 * l + s] : R(0);
+  }
+  const int di = n1 * hk;
+  const int sim = max(lane - di, 0), sip = min(lane + di, 31);
+  const int sjm = max(lane - hk, 0), sjp = min(lane + hk, 31);
+  const int skm = max(lane - 1, 0), skp = min(lane + 1, 31);
+  for (int sw = 0; sw < sweeps; ++sw) {
+#pragma unroll
+    for (int color = 0; color < 2; ++color) {
+      const int sc = (color - i - j) & 1;
+      const R pub = sc ? p[0] : p[1];
+      const R vim = __shfl_sync(0xffffffffu, pub, sim), vip = __shfl_sync(0xffffffffu, pub, sip);
+      const R vjm = __shfl_sync(0xffffffffu, pub, sjm), vjp = __shfl_sync(0xffffffffu, pub, sjp);
+      const R vkm = __shfl_sync(0xffffffffu, pub, skm), vkp = __shfl_sync(0xffffffffu, pub, skp);
+      const R pv = sc ? p[1] : p[0];
+      const R q0 = i > 0 ? vim : pv, q1 = i < n0 - 1 ? vip : pv;
+      const R q2 = j > 0 ? vjm : pv, q3 = j < n1 - 1 ? vjp : pv;
+      const R q4 = sc ? p[0] : (h > 0 ? vkm : pv);
+      const R q5 = sc ? (h < hk - 1 ? vkp : pv) : p[1];
+      const R bxl = sc ? cx0[1] : cx0[0], bxu = sc ? cx1[1] : cx1[0];
+      const R byl = sc ? cy0[1] : cy0[0], byu = sc ? cy1[1] : cy1[0];
+      const R bzl = sc ? cz0[1] : cz0[0], bzu = sc ? cz1[1] : cz1[0];
+      const R d = sc ? cd[1] : cd[0], bb = sc ? cb[1] : cb[0];
+      R res;
+      if (flux) {
+        R sum = bxl * (pv - q0);
+        sum += bxu * (pv - q1);
+        sum += byl * (pv - q2);
+        sum += byu * (pv - q3);
+        sum += bzl * (pv - q4);
+        sum += bzu * (pv - q5);
+        res = bb - sum;
+      } else {
+        R sum = bxl * q0;
+        sum += bxu * q1;
+        sum += byl * q2;
+        sum += byu * q3;
+        sum += bzl * q4;
+        sum += bzu * q5;
+        res = bb - (d * pv - sum);
+      }
+      const R nv = (act && d > R(0)) ? pv + omega * res / d : pv;
+      if (sc) p[1] = nv;
+      else p[0] = nv;
+    }
+  }
+  if (act) {
+    P[2 * l] = p[0];
+    P[2 * l + 1] = p[1];
+  }
 }
 
 // one half-sweep (cells of `color`) over a level with nt threads starting at tid
@@ -837,20 +926,81 @@ __global__ void __launch_bounds__(BT_NT) k_bottom(BottomArgs<T, TB> a) {
     Pc = reinterpret_cast<AccT*>((reinterpret_cast<uintptr_t>(end) + 15) & ~uintptr_t(15));
   }
   // ---- load faces of every level and b of the top level; zero p
-  for (int l = 0; l < nl; ++l) {
-    const BottomLevel& L = a.L[l];
-    const LvPtr q = ptrs(l);
-    const int n = L.n0 * L.n1 * L.n2;
-    bt_load(q.X, reinterpret_cast<const T*>(L.bx), (L.n0 + 1) * L.n1 * L.n2, 1.f, tid);
-    bt_load(q.Y, reinterpret_cast<const T*>(L.by), L.n0 * (L.n1 + 1) * L.n2, 1.f, tid);
-    bt_load(q.Z, reinterpret_cast<const T*>(L.bz), L.n0 * L.n1 * (L.n2 + 1), 1.f, tid);
-    for (int e = tid; e < n; e += BT_NT) q.P[e] = 0.f;
+  if (a.bulk) {
+    // one thread issues a bulk copy per array (the host checked that every
+    // array is fp32, 16-byte aligned and a multiple of 16 bytes long); all
+    // complete on one mbarrier, waited on with a bound
+    __shared__ __align__(8) uint64_t bt_bar;
+    __shared__ int bt_fail;
+    if (tid == 0) {
+      bt_fail = 0;
+      unsigned bytes = 4u * (unsigned)(a.L[0].n0 * a.L[0].n1 * a.L[0].n2);
+      for (int l = 0; l < nl; ++l) {
+        const BottomLevel& L = a.L[l];
+        bytes += 4u * (unsigned)((L.n0 + 1) * L.n1 * L.n2 + L.n0 * (L.n1 + 1) * L.n2 + L.n0 * L.n1 * (L.n2 + 1));
+      }
+      const unsigned bar = smem_u32(&bt_bar);
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+      auto bulk = [&](float* dst, const void* src, int count) {
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                smem_u32(dst)),
+            "l"(reinterpret_cast<uint64_t>(src)), "r"(4 * count), "r"(bar)
+            : "memory");
+      };
+      for (int l = 0; l < nl; ++l) {
+        const BottomLevel& L = a.L[l];
+        const LvPtr q = ptrs(l);
+        bulk(q.X, L.bx, (L.n0 + 1) * L.n1 * L.n2);
+        bulk(q.Y, L.by, L.n0 * (L.n1 + 1) * L.n2);
+        bulk(q.Z, L.bz, L.n0 * L.n1 * (L.n2 + 1));
+      }
+      bulk(ptrs(0).B, a.b, a.L[0].n0 * a.L[0].n1 * a.L[0].n2);
+    }
+    for (int l = 0; l < nl; ++l) {
+      const LvPtr q = ptrs(l);
+      const int n = a.L[l].n0 * a.L[l].n1 * a.L[l].n2;
+      for (int e = tid; e < n; e += BT_NT) q.P[e] = 0.f;
+    }
+    __syncthreads();  // barrier initialised before anyone waits on it
+    {
+      unsigned it = 0;
+      while (!mbar_try_wait(&bt_bar, 0)) {
+        if (++it > kTmaWaitLimit) {
+          bt_fail = 1;
+          break;
+        }
+      }
+    }
+    __syncthreads();
+    if (bt_fail) {
+      if (tid == 0 && a.st) {
+        a.st->status = ST_TMA_TIMEOUT;
+        a.st->done = 1;
+      }
+      unsigned it = 0;  // give the copies in flight a last bounded chance to land
+      while (!mbar_try_wait(&bt_bar, 0) && ++it < kTmaWaitLimit) {
+      }
+      return;
+    }
+  } else {
+    for (int l = 0; l < nl; ++l) {
+      const BottomLevel& L = a.L[l];
+      const LvPtr q = ptrs(l);
+      const int n = L.n0 * L.n1 * L.n2;
+      bt_load(q.X, reinterpret_cast<const T*>(L.bx), (L.n0 + 1) * L.n1 * L.n2, 1.f, tid);
+      bt_load(q.Y, reinterpret_cast<const T*>(L.by), L.n0 * (L.n1 + 1) * L.n2, 1.f, tid);
+      bt_load(q.Z, reinterpret_cast<const T*>(L.bz), L.n0 * L.n1 * (L.n2 + 1), 1.f, tid);
+      for (int e = tid; e < n; e += BT_NT) q.P[e] = 0.f;
+    }
+    {
+      const LvPtr q = ptrs(0);
+      bt_load(q.B, a.b, a.L[0].n0 * a.L[0].n1 * a.L[0].n2, a.b_scale ? *a.b_scale : 1.f, tid);
+    }
+    __syncthreads();
   }
-  {
-    const LvPtr q = ptrs(0);
-    bt_load(q.B, a.b, a.L[0].n0 * a.L[0].n1 * a.L[0].n2, a.b_scale ? *a.b_scale : 1.f, tid);
-  }
-  __syncthreads();
   const float om = a.omega;
   // ---- down: pre-smoothing, residual, restriction
   for (int l = 0; l < nl - 1; ++l) {
@@ -929,7 +1079,9 @@ __global__ void __launch_bounds__(BT_NT) k_bottom(BottomArgs<T, TB> a) {
     __syncthreads();
     const bool one_warp = n <= 256;
     const AccT omc = (AccT)om;
-    if (!one_warp || tid < 32) {
+    if (n <= 64 && (L.n2 & 1) == 0) {
+      if (tid < 32) bt_coarsest_regs<AccT>(L, Pc, q.B, q.X, q.Y, q.Z, omc, a.coarsest, a.flux, tid);
+    } else if (!one_warp || tid < 32) {
       const int nt = one_warp ? 32 : BT_NT;
       for (int sw = 0; sw < a.coarsest; ++sw) {
         for (int color = 0; color < 2; ++color) {
@@ -1486,6 +1638,19 @@ int launch_bottom(pf_mg_plan* P, const TB* b, const float* b_scale, bool want_me
   a.st = ST(P);
   a.want_mean = want_mean ? 1 : 0;
   a.mixed = mixed(P) ? 1 : 0;
+  a.bulk = 0;
+  if constexpr (std::is_same<T, float>::value && std::is_same<TB, float>::value) {
+    bool ok = b_scale == nullptr && aligned16(b) && ((size_t)ncells(P->d.lev[lb]) * 4) % 16 == 0;
+    for (int l = 0; l < a.nl && ok; ++l) {
+      const BottomLevel& L = a.L[l];
+      const long long nf[3] = {(long long)(L.n0 + 1) * L.n1 * L.n2, (long long)L.n0 * (L.n1 + 1) * L.n2,
+                               (long long)L.n0 * L.n1 * (L.n2 + 1)};
+      const void* ptr[3] = {L.bx, L.by, L.bz};
+      ok = ok && ((long long)L.n0 * L.n1 * L.n2) % 4 == 0;  // P and B keep every shared offset 16-byte aligned
+      for (int c = 0; c < 3; ++c) ok = ok && aligned16(ptr[c]) && (nf[c] * 4) % 16 == 0;
+    }
+    a.bulk = ok ? 1 : 0;
+  }
   if (mixed(P)) k_bottom<T, TB, double><<<1, BT_NT, P->bottom_smem, s>>>(a);
   else k_bottom<T, TB, float><<<1, BT_NT, P->bottom_smem, s>>>(a);
   PF_LAUNCHED();

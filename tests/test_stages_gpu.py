@@ -311,3 +311,25 @@ def test_g2p_packed_matches_unpaired(flags):
     assert np.array_equal(pa[:, 3].view(np.int32), pb[:, 3].view(np.int32))
     assert np.abs(pa[:, :3] - pb[:, :3]).max() <= 4 * np.spacing(np.float32(np.abs(pa[:, :3]).max()))
     assert np.abs(va[:, :3] - vb[:, :3]).max() <= 4 * np.spacing(np.float32(np.abs(va[:, :3]).max()))
+
+
+@pytest.mark.parametrize("sweeps", [0, 2, 3, 4])
+def test_extrapolation_level_passes_equal_tiled_sweeps(sweeps):
+    """pf_extrapolate computes level by level in place when known arrays are
+    given and with tiled shared-memory sweeps when they are NULL: bit-equal."""
+    res = (30, 18, 40)
+    g = N.grid(res, np.float32(1 / 30))
+    rng = np.random.default_rng(13)
+    fs = ((31, 18, 40), (30, 19, 40), (30, 18, 41))
+    liq = torch.tensor((rng.random(res) < 0.1).astype(np.int32), device=DEV)
+    u = [torch.tensor(rng.standard_normal(s).astype(np.float32), device=DEV) for s in fs]
+    a = [torch.full(s, np.nan, device=DEV) for s in fs]
+    b = [torch.full(s, np.nan, device=DEV) for s in fs]
+    kn = [torch.full(s, -5, dtype=torch.int32, device=DEV) for s in fs]
+    N.call("pf_extrapolate", C.byref(g), *(t.data_ptr() for t in u), liq.data_ptr(), sweeps,
+           *(t.data_ptr() for t in a), None, None, None, N.stream())
+    N.call("pf_extrapolate", C.byref(g), *(t.data_ptr() for t in u), liq.data_ptr(), sweeps,
+           *(t.data_ptr() for t in b), *(t.data_ptr() for t in kn), N.stream())
+    for x, y, k in zip(a, b, kn):
+        assert torch.equal(x.view(torch.int32), y.view(torch.int32))
+        assert set(torch.unique(k).tolist()) <= {0, 1}
