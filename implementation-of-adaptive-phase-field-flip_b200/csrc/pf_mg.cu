@@ -465,8 +465,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase) {
 
 constexpr unsigned kTmaWaitLimit = 1u << 22;
 
-template <int TI>
-__global__ void __launch_bounds__(SW_NT) k_rb_tile_tma(const __grid_constant__ TileMaps maps, SweepArgs<float, float> a) {
+template <int TI, int NT>
+__global__ void __launch_bounds__(NT) k_rb_tile_tma(const __grid_constant__ TileMaps maps, SweepArgs<float, float> a) {
   if (is_done(a.st)) return;
   using D = TmaDims<TI>;
   extern __shared__ __align__(128) unsigned char tsm_raw[];
@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(SW_NT) k_rb_tile_tma(const __grid_constant__ T
     tma_load_3d(sZ, &maps.z, x, j0 - 1, i0 - 1, bar);
   }
   if (!load_p)
-    for (int e = tid; e < D::PN; e += SW_NT) sP[e] = 0.f;
+    for (int e = tid; e < D::PN; e += NT) sP[e] = 0.f;
   __syncthreads();  // barrier initialised before anyone waits on it
   {
     unsigned it = 0;
@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(SW_NT) k_rb_tile_tma(const __grid_constant__ T
     return;
   }
   if (a.pc) {  // prolongation folded into the staged p
-    for (int e = tid; e < D::PN; e += SW_NT) {
+    for (int e = tid; e < D::PN; e += NT) {
       const int c = e % TM_W, t = e / TM_W, r = t % D::PJ, q = t / D::PJ;
       const int i = i0 - 2 + q, j = j0 - 2 + r, k = k0 - TM_X0 + c;
       if (i >= 0 && i < n0 && j >= 0 && j < n1 && k >= 0 && k < n2)
@@ -548,22 +548,37 @@ __global__ void __launch_bounds__(SW_NT) k_rb_tile_tma(const __grid_constant__ T
     if (ok) *pp = v;
   };
   const int c1 = a.first_color, c2 = c1 ^ 1;
+  // colour 1 on the tile and its 1-cell ring.  Ring row (q, r) holds 34 cells
+  // k0-1 .. k0+32; the 16 of colour c1 inside k0 .. k0+31 go to the 16 lanes
+  // of a half-warp, and the one at k0-1 or k0+32 (the two have opposite
+  // colours) to one thread per row.
   {
-    constexpr int HALF = (SW_TK + 2) / 2;  // 17 cells of one colour per ring row
-    for (int e = tid; e < D::CI * D::CJ * HALF; e += SW_NT) {
-      const int h = e % HALF, row = e / HALF, r = row % D::CJ, q = row / D::CJ;
+    constexpr int ROWS = D::CI * D::CJ;
+    const int h = tid & 15;
+    for (int row = tid >> 4; row < ROWS; row += NT / 16) {
+      const int q = row / D::CJ, r = row - q * D::CJ;
       const int i = i0 - 1 + q, j = j0 - 1 + r;
-      const int par = (c1 - i - j - (k0 - 1)) & 1;
-      const int c = 2 * h + par, k = k0 - 1 + c;
+      const int par = (c1 - i - j - k0) & 1;
+      const int c = 1 + 2 * h + par, k = k0 - 1 + c;
+      if (i < 0 || i >= n0 || j < 0 || j >= n1 || k >= n2) continue;
+      relax(q, r, c);
+    }
+    for (int row = tid; row < ROWS; row += NT) {
+      const int q = row / D::CJ, r = row - q * D::CJ;
+      const int i = i0 - 1 + q, j = j0 - 1 + r;
+      const bool lower = ((c1 - i - j - (k0 - 1)) & 1) == 0;  // k0-1 has colour c1
+      const int c = lower ? 0 : SW_TK + 1, k = k0 - 1 + c;
       if (i < 0 || i >= n0 || j < 0 || j >= n1 || k < 0 || k >= n2) continue;
       relax(q, r, c);
     }
   }
   __syncthreads();
+  // colour 2 on the tile: 16 cells of the colour per row, a half-warp per row
   {
-    constexpr int HALF = SW_TK / 2;
-    for (int e = tid; e < TI * SW_TJ * HALF; e += SW_NT) {
-      const int h = e % HALF, row = e / HALF, r = row % SW_TJ, q = row / SW_TJ;
+    constexpr int ROWS = TI * SW_TJ;
+    const int h = tid & 15;
+    for (int row = tid >> 4; row < ROWS; row += NT / 16) {
+      const int q = row >> 3, r = row & 7;  // SW_TJ == 8
       const int i = i0 + q, j = j0 + r;
       const int par = (c2 - i - j - k0) & 1;
       const int c = 2 * h + par, k = k0 + c;
@@ -573,8 +588,8 @@ __global__ void __launch_bounds__(SW_NT) k_rb_tile_tma(const __grid_constant__ T
   }
   __syncthreads();
   double msum = 0.0;
-  for (int e = tid; e < TI * SW_TJ * SW_TK; e += SW_NT) {
-    const int c = e % SW_TK, t = e / SW_TK, r = t % SW_TJ, q = t / SW_TJ;
+  for (int e = tid; e < TI * SW_TJ * SW_TK; e += NT) {
+    const int c = e & 31, r = (e >> 5) & 7, q = e >> 8;  // SW_TK == 32, SW_TJ == 8
     const int i = i0 + q, j = j0 + r, k = k0 + c;
     if (i >= n0 || j >= n1 || k >= n2) continue;
     const float v = sP[((q + 2) * D::PJ + (r + 2)) * TM_W + (c + TM_X0)];
@@ -582,7 +597,7 @@ __global__ void __launch_bounds__(SW_NT) k_rb_tile_tma(const __grid_constant__ T
     if (a.partials) msum += (double)v;
   }
   if (a.partials) {
-    const double bs = block_sum<SW_NT>(msum, sred);
+    const double bs = block_sum<NT>(msum, sred);
     const int nb = gridDim.x * gridDim.y * gridDim.z;
     const int bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
     __shared__ bool s_last;
@@ -595,8 +610,8 @@ __global__ void __launch_bounds__(SW_NT) k_rb_tile_tma(const __grid_constant__ T
     if (s_last) {
       __threadfence();
       double v = 0.0;
-      for (int q = tid; q < nb; q += SW_NT) v += __ldcg(a.partials + q);
-      v = block_sum<SW_NT>(v, sred);
+      for (int q = tid; q < nb; q += NT) v += __ldcg(a.partials + q);
+      v = block_sum<NT>(v, sred);
       if (tid == 0) {
         a.st->sum_last = v;
         a.st->c_shift = (float)(-(v / (double)a.n_total));
@@ -1554,14 +1569,13 @@ bool encode3d(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint64
 }
 
 // TMA staging of a level: fp32 storage, rows a multiple of 4 floats, padded z-faces
-template <class T, class TB>
+template <int TI, class T, class TB>
 bool tma_maps(pf_mg_plan* P, int lv, const T* p_in, const TB* b, const float* b_scale, const LV<T>& V, TileMaps* m) {
   if constexpr (!std::is_same<T, float>::value || !std::is_same<TB, float>::value) {
     return false;
   } else {
     const pf_mg_level& L = P->d.lev[lv];
     if (b_scale || !L.bz_pad || L.nz % 4 != 0 || L.bz_pitch % 8 != 0) return false;
-    constexpr int TI = 4;
     const uint64_t n0 = L.nx, n1 = L.ny, n2 = L.nz;
     const float* pm = p_in ? p_in : V.p0;
     return encode3d(&m->p, pm, n2, n1, n0, n2, n1 * n2, TM_W, SW_TJ + 4, TI + 4) &&
@@ -1596,8 +1610,16 @@ int launch_sweep(pf_mg_plan* P, int lv, const T* p_in, bool zero_in, T* p_out, c
   dim3 grid((L.nz + SW_TK - 1) / SW_TK, (L.ny + SW_TJ - 1) / SW_TJ, (L.nx + TI - 1) / TI);
   if constexpr (std::is_same<T, float>::value && std::is_same<TB, float>::value) {
     TileMaps maps;
-    if (P->use_tma && tma_maps<T, TB>(P, lv, p_in, b, b_scale, V, &maps)) {
-      k_rb_tile_tma<TI><<<grid, SW_NT, TmaDims<TI>::SMEM, s>>>(maps, a);
+    // large levels: 8-plane tiles (1.33 relaxations and 44 staged bytes per
+    // cell instead of 1.5 and 55), 512 threads, two CTAs per SM
+    if (P->use_tma && L.nx >= 128 && tma_maps<8, T, TB>(P, lv, p_in, b, b_scale, V, &maps)) {
+      const dim3 g8(grid.x, grid.y, (L.nx + 7) / 8);
+      k_rb_tile_tma<8, 512><<<g8, 512, TmaDims<8>::SMEM, s>>>(maps, a);
+      PF_LAUNCHED();
+      return PF_OK;
+    }
+    if (P->use_tma && tma_maps<TI, T, TB>(P, lv, p_in, b, b_scale, V, &maps)) {
+      k_rb_tile_tma<TI, SW_NT><<<grid, SW_NT, TmaDims<TI>::SMEM, s>>>(maps, a);
       PF_LAUNCHED();
       return PF_OK;
     }
@@ -1922,7 +1944,9 @@ template <class T> cudaError_t set_smem_attrs() {
   chk(cudaFuncSetAttribute(k_bottom<T, T, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   chk(cudaFuncSetAttribute(k_rb_tile<T, float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile));
   chk(cudaFuncSetAttribute(k_rb_tile<T, T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile));
-  chk(cudaFuncSetAttribute(k_rb_tile_tma<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TmaDims<4>::SMEM));
+  chk(cudaFuncSetAttribute(k_rb_tile_tma<4, SW_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)TmaDims<4>::SMEM));
+  chk(cudaFuncSetAttribute(k_rb_tile_tma<8, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TmaDims<8>::SMEM));
   return e;
 }
 

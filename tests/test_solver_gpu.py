@@ -85,10 +85,10 @@ def test_hierarchy_matches_oracle_bitwise():
             assert np.array_equal(getattr(L, name).numpy(), o.level_array(lv, name)), (lv, name)
 
 
+@pytest.mark.parametrize("res", [(24, 40, 36), (136, 44, 36)])  # ragged tiles; the second takes 8-plane tiles
 @pytest.mark.parametrize("stencil", ["reference", "flux"])
-def test_smoother_matches_oracle(stencil):
+def test_smoother_matches_oracle(stencil, res):
     rng = np.random.default_rng(5)
-    res = (24, 40, 36)  # not multiples of the tile, odd level count
     bx, by, bz, _, _ = scenes.solve_problem(res, seed=4)
     g = MGPCG(res, DEV, stencil=stencil)
     g.build_hierarchy(dev(bx), dev(by), dev(bz))
