@@ -465,65 +465,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase) {
 
 constexpr unsigned kTmaWaitLimit = 1u << 22;
 
+// One staged tile of the red-black sweep: prolongation folded into the staged
+// p (first post-sweep), colour 1 on the tile and its ring, colour 2 on the
+// tile, write-back of the tile to p_out (msum += the written values).
 template <int TI, int NT>
-__global__ void __launch_bounds__(NT) k_rb_tile_tma(const __grid_constant__ TileMaps maps, SweepArgs<float, float> a) {
-  if (is_done(a.st)) return;
+__device__ __forceinline__ void tma_tile_sweep(float* sP, const float* sB, const float* sX, const float* sY,
+                                               const float* sZ, const SweepArgs<float, float>& a, int k0, int j0,
+                                               int i0, double& msum) {
   using D = TmaDims<TI>;
-  extern __shared__ __align__(128) unsigned char tsm_raw[];
-  unsigned char* tsm = tsm_raw + ((128u - (smem_u32(tsm_raw) & 127u)) & 127u);
-  float* sP = reinterpret_cast<float*>(tsm);
-  float* sB = reinterpret_cast<float*>(tsm + D::OFF_B);
-  float* sX = reinterpret_cast<float*>(tsm + D::OFF_X);
-  float* sY = reinterpret_cast<float*>(tsm + D::OFF_Y);
-  float* sZ = reinterpret_cast<float*>(tsm + D::OFF_Z);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(tsm + D::OFF_BAR);
-  __shared__ double sred[40];
-  __shared__ int s_fail;
-
   const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
-  const int k0 = blockIdx.x * SW_TK, j0 = blockIdx.y * SW_TJ, i0 = blockIdx.z * TI;
   const int tid = threadIdx.x;
   const long long sI = (long long)n1 * n2;
   const int hn1 = n1 >> 1, hn2 = n2 >> 1;
-  const bool load_p = !a.zero_in;
-
-  if (tid == 0) {
-    s_fail = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    const unsigned bytes = 4u * (unsigned)((load_p ? D::PN : 0) + D::BN + D::XN + D::YN + D::ZN);
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-    const int x = k0 - TM_X0;
-    if (load_p) tma_load_3d(sP, &maps.p, x, j0 - 2, i0 - 2, bar);
-    tma_load_3d(sB, &maps.b, x, j0 - 1, i0 - 1, bar);
-    tma_load_3d(sX, &maps.x, x, j0 - 1, i0 - 1, bar);
-    tma_load_3d(sY, &maps.y, x, j0 - 1, i0 - 1, bar);
-    tma_load_3d(sZ, &maps.z, x, j0 - 1, i0 - 1, bar);
-  }
-  if (!load_p)
-    for (int e = tid; e < D::PN; e += NT) sP[e] = 0.f;
-  __syncthreads();  // barrier initialised before anyone waits on it
-  {
-    unsigned it = 0;
-    while (!mbar_try_wait(bar, 0)) {
-      if (++it > kTmaWaitLimit) {
-        s_fail = 1;
-        break;
-      }
-    }
-  }
-  __syncthreads();
-  if (s_fail) {
-    if (tid == 0 && a.st) {
-      a.st->status = ST_TMA_TIMEOUT;
-      a.st->done = 1;
-    }
-    unsigned it = 0;  // give the copies in flight a last bounded chance to land
-    while (!mbar_try_wait(bar, 0) && ++it < kTmaWaitLimit) {
-    }
-    return;
-  }
   if (a.pc) {  // prolongation folded into the staged p
     for (int e = tid; e < D::PN; e += NT) {
       const int c = e % TM_W, t = e / TM_W, r = t % D::PJ, q = t / D::PJ;
@@ -587,7 +540,6 @@ __global__ void __launch_bounds__(NT) k_rb_tile_tma(const __grid_constant__ Tile
     }
   }
   __syncthreads();
-  double msum = 0.0;
   for (int e = tid; e < TI * SW_TJ * SW_TK; e += NT) {
     const int c = e & 31, r = (e >> 5) & 7, q = e >> 8;  // SW_TK == 32, SW_TJ == 8
     const int i = i0 + q, j = j0 + r, k = k0 + c;
@@ -596,6 +548,13 @@ __global__ void __launch_bounds__(NT) k_rb_tile_tma(const __grid_constant__ Tile
     a.p_out[i * sI + (long long)j * n2 + k] = v;
     if (a.partials) msum += (double)v;
   }
+}
+
+// mean of p_out over the grid: one partial per CTA, the last CTA sums them in
+// order and stores the shift in the solver state
+template <int NT>
+__device__ __forceinline__ void sweep_mean_finish(const SweepArgs<float, float>& a, double msum, double* sred) {
+  const int tid = threadIdx.x;
   if (a.partials) {
     const double bs = block_sum<NT>(msum, sred);
     const int nb = gridDim.x * gridDim.y * gridDim.z;
@@ -620,6 +579,71 @@ __global__ void __launch_bounds__(NT) k_rb_tile_tma(const __grid_constant__ Tile
     }
   }
 }
+
+template <int TI, int NT>
+__global__ void __launch_bounds__(NT) k_rb_tile_tma(const __grid_constant__ TileMaps maps, SweepArgs<float, float> a) {
+  if (is_done(a.st)) return;
+  using D = TmaDims<TI>;
+  extern __shared__ __align__(128) unsigned char tsm_raw[];
+  unsigned char* tsm = tsm_raw + ((128u - (smem_u32(tsm_raw) & 127u)) & 127u);
+  float* sP = reinterpret_cast<float*>(tsm);
+  float* sB = reinterpret_cast<float*>(tsm + D::OFF_B);
+  float* sX = reinterpret_cast<float*>(tsm + D::OFF_X);
+  float* sY = reinterpret_cast<float*>(tsm + D::OFF_Y);
+  float* sZ = reinterpret_cast<float*>(tsm + D::OFF_Z);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tsm + D::OFF_BAR);
+  __shared__ double sred[40];
+  __shared__ int s_fail;
+
+  const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
+  const int k0 = blockIdx.x * SW_TK, j0 = blockIdx.y * SW_TJ, i0 = blockIdx.z * TI;
+  const int tid = threadIdx.x;
+  const long long sI = (long long)n1 * n2;
+  const int hn1 = n1 >> 1, hn2 = n2 >> 1;
+  const bool load_p = !a.zero_in;
+
+  if (tid == 0) {
+    s_fail = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    const unsigned bytes = 4u * (unsigned)((load_p ? D::PN : 0) + D::BN + D::XN + D::YN + D::ZN);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    const int x = k0 - TM_X0;
+    if (load_p) tma_load_3d(sP, &maps.p, x, j0 - 2, i0 - 2, bar);
+    tma_load_3d(sB, &maps.b, x, j0 - 1, i0 - 1, bar);
+    tma_load_3d(sX, &maps.x, x, j0 - 1, i0 - 1, bar);
+    tma_load_3d(sY, &maps.y, x, j0 - 1, i0 - 1, bar);
+    tma_load_3d(sZ, &maps.z, x, j0 - 1, i0 - 1, bar);
+  }
+  if (!load_p)
+    for (int e = tid; e < D::PN; e += NT) sP[e] = 0.f;
+  __syncthreads();  // barrier initialised before anyone waits on it
+  {
+    unsigned it = 0;
+    while (!mbar_try_wait(bar, 0)) {
+      if (++it > kTmaWaitLimit) {
+        s_fail = 1;
+        break;
+      }
+    }
+  }
+  __syncthreads();
+  if (s_fail) {
+    if (tid == 0 && a.st) {
+      a.st->status = ST_TMA_TIMEOUT;
+      a.st->done = 1;
+    }
+    unsigned it = 0;  // give the copies in flight a last bounded chance to land
+    while (!mbar_try_wait(bar, 0) && ++it < kTmaWaitLimit) {
+    }
+    return;
+  }
+  double msum = 0.0;
+  tma_tile_sweep<TI, NT>(sP, sB, sX, sY, sZ, a, k0, j0, i0, msum);
+  sweep_mean_finish<NT>(a, msum, sred);
+}
+
 
 // --------------------------------------------------------------- residual + restriction
 // coarse b = rscale * sum over the 8 fine cells of (b - A p)  (pfflip/poisson.py:91-102, :166-175)
@@ -1500,6 +1524,7 @@ struct pf_mg_plan {
   float lp_scale[PF_MG_MAX_LEVELS];
   int lb;              // first level solved by the single-CTA bottom kernel (nlev = none)
   bool use_tma;        // stage fp32 smoother tiles with TMA where the level allows it
+  int sms;             // multiprocessors of the plan's device (persistent sweep grid)
   size_t bottom_smem;  // dynamic shared memory of the bottom kernel
   cudaStream_t cap_stream;
   cudaGraphExec_t exec[2];
@@ -1997,6 +2022,13 @@ int pf_mg_plan_create(const pf_mg_desc* desc, pf_mg_plan** out) {
   {
     const char* env = std::getenv("PFFLIP_NO_TMA");
     P->use_tma = !(env && env[0] == '1');
+  }
+  {
+    int dev = 0;
+    P->sms = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&P->sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaGetLastError();
+    if (P->sms <= 0) P->sms = kNumSMs;
   }
   for (int lv = 0; lv < desc->nlev; ++lv) {
     const pf_mg_level& L = desc->lev[lv];

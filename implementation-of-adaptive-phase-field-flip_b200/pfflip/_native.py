@@ -97,6 +97,13 @@ SIGNATURES = {
                                                                           C.POINTER(_F), _I32, _I32, _VP,
                                                                           C.c_size_t, _VP]),
     "pf_particle_max_speed": (C.c_int, [_I64, _VP, _VP, _VP, _VP]),
+    "pf_droplet_classify": (C.c_int, [_G, _I64, _VP, _VP, _VP, _VP, _F, _F, _F, _F, _F, C.c_uint32, _VP, _VP]),
+    "pf_velocity_gradient": (C.c_int, [_G, _VP, _VP, _VP, _VP, _VP]),
+    "pf_spray_emit": (C.c_int, [_G, _I64, _VP, _VP, _VP, _VP, _VP, _F, _F, _F, _F, _F, _F, C.c_uint32, _VP, _VP]),
+    "pf_droplet_advance": (C.c_int, [_G, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _F, C.POINTER(_F), _F, _F, _F, _F, _F,
+                                     C.POINTER(_F), C.POINTER(_F), _I32, _VP]),
+    "pf_spray_rasterize": (C.c_int, [_I64, _VP, _VP, _VP, _I32, _I32, _I32, _F, _VP]),
+    "pf_permute_f32": (C.c_int, [_I64, _VP, _VP, _VP, _VP]),
     "pf_apply_A": (C.c_int, [_G, _VP, _VP, _VP, _VP, _VP, _VP, _I32, _VP]),
     "pf_mg_partials_count": (C.c_int64, []),
     "pf_mg_level_count": (C.c_int32, [_I32, _I32, _I32, _I32, C.POINTER(_I32)]),

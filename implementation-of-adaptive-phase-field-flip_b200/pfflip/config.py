@@ -51,8 +51,7 @@ class Config:
     # liquid velocity extrapolation depth in cells
     extrap_cells: int = 3
 
-    # escaped-particle / spray parameters.  The droplet stage is not part of this
-    # implementation: they are accepted so reference configurations construct.
+    # escaped-particle / droplet / spray parameters (pfflip/config.py, paper 3.4, 7)
     droplets: bool = True
     delta_phi: float = 0.2
     droplet_radius_mean: float = 0.25

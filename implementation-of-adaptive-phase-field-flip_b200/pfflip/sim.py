@@ -15,13 +15,17 @@ vel_star copy + forces       pf_save_and_force
 ``_project``                 pf_project
 ``_max_divergence``          pf_max_divergence
 ``_extrapolate_liquid_vel.`` pf_extrapolate
-``_g2p`` + ``_advect``       pf_g2p_advect (one fused pass inside ``step``)
+``_g2p`` + ``_advect``       pf_g2p_advect_packed (one fused pass inside
+                             ``step`` when droplets are off)
+``_droplets``                pf_droplet_classify, pf_velocity_gradient,
+                             pf_spray_emit, pf_droplet_advance
+``rasterize_spray``          pf_spray_rasterize
 ==========================  ===============================================
 
 Particles live on the device as two float4 streams sorted by cell (see
-include/pfflip.h); ``px``, ``pv``, ``ptype``, ``pmass``, ``pstate`` present them
-in the caller's original order.  The droplet stage (``cfg.droplets``) is not
-part of this implementation and is skipped with a warning.
+include/pfflip.h); ``px``, ``pv``, ``ptype``, ``pmass``, ``pstate``, ``pdrop_r``
+present them in the caller's original order.  With ``cfg.droplets`` the step
+keeps the reference's order G2P -> extrapolation -> droplets -> advection.
 """
 
 from __future__ import annotations
@@ -29,7 +33,6 @@ from __future__ import annotations
 import ctypes as C
 import math
 import time
-import warnings
 
 import numpy as np
 import torch
@@ -89,6 +92,8 @@ class ParticleField:
                             torch.tensor(cfg.rho_g, dtype=torch.float32, device=s.dev))
         elif k == "prad":
             v = torch.full_like(flags, 0, dtype=torch.float32) + float(np.float32(s.cfg.r_p))
+        elif k == "pdrop_r":
+            v = s._drop_r
         out = torch.empty_like(v)
         out[ids] = v
         return out
@@ -171,7 +176,6 @@ class Simulator:
         self.time = 0.0
         self.step_index = 0
         self.stats: list[dict] = []
-        self._warned_droplets = False
         self._marks = None  # per-stage CUDA events when stage timing is on
         self._g2p_ws = None  # k-paired face fields of the G2P/advection pass
 
@@ -179,6 +183,14 @@ class Simulator:
         self.pv = ParticleField(self, "vel")
         self.ptype = ParticleField(self, "ptype")
         self.pstate = ParticleField(self, "pstate")
+        self.pdrop_r = ParticleField(self, "pdrop_r")
+        # spray density field at spray_resolution_factor x the grid (pfflip/sim.py:94-98)
+        f = max(1, int(cfg.spray_resolution_factor))
+        self.spray_res = tuple(n * f for n in self.res)
+        self.dx_spray = cfg.dx / f
+        self.spray_density = None  # float16, allocated by the first rasterize_spray()
+        self.shear = None
+        self._counters = torch.zeros(4, dtype=torch.int32, device=self.dev)
         self.pmass = ParticleField(self, "pmass")
         self.prad = ParticleField(self, "prad")
 
@@ -208,6 +220,8 @@ class Simulator:
         v4[:, :3].copy_(vel, non_blocking=True)
         p4.view(torch.int32)[:, 3].copy_((ptype == 1).to(torch.int32), non_blocking=True)
         v4.view(torch.int32)[:, 3] = torch.arange(n, dtype=torch.int32, device=dev)
+        if self.cfg.droplets:
+            self._drop_r.zero_()
         self._sort()
 
     def read_particles(self, pos_out=None, vel_out=None):
@@ -227,6 +241,8 @@ class Simulator:
 
     def _alloc_particles(self, n):
         dev = self.dev
+        self._drop_r = torch.zeros(n, dtype=torch.float32, device=dev)
+        self._drop_r_alt = torch.empty_like(self._drop_r)
         self._pos4 = torch.empty((n, 4), dtype=torch.float32, device=dev)
         self._vel4 = torch.empty((n, 4), dtype=torch.float32, device=dev)
         self._pos4_alt = torch.empty_like(self._pos4)
@@ -253,6 +269,10 @@ class Simulator:
                self._cell_start.data_ptr(), self._sort_ws.data_ptr(), self._sort_ws.numel(), N.stream())
         self._pos4, self._pos4_alt = self._pos4_alt, self._pos4
         self._vel4, self._vel4_alt = self._vel4_alt, self._vel4
+        if self.cfg.droplets:  # the droplet radius follows its particle
+            N.call("pf_permute_f32", n, self._perm.data_ptr(), self._drop_r.data_ptr(), self._drop_r_alt.data_ptr(),
+                   N.stream())
+            self._drop_r, self._drop_r_alt = self._drop_r_alt, self._drop_r
 
     # ------------------------------------------------------------------ timing
     def enable_stage_timing(self, on: bool = True):
@@ -304,11 +324,22 @@ class Simulator:
         self._project(dt)
         mark("divergence")
         self._divergence_async()
-        mark("extrapolate")
-        self._extrapolate_liquid_velocity()
-        self._droplets(dt)
-        mark("g2p_advect")
-        self._g2p_advect(dt, do_g2p=True, do_advect=True)
+        if self.cfg.droplets:
+            # the reference's order (pfflip/sim.py:182-185): droplet
+            # conversions sit between G2P and advection, so the passes split
+            mark("g2p_advect")
+            self._g2p()
+            mark("extrapolate")
+            self._extrapolate_liquid_velocity()
+            mark("droplets")
+            self._droplets(dt)
+            mark("g2p_advect")
+            self._advect(dt)
+        else:
+            mark("extrapolate")
+            self._extrapolate_liquid_velocity()
+            mark("g2p_advect")
+            self._g2p_advect(dt, do_g2p=True, do_advect=True)
         mark("<end>")
         div_after = float(self._scal[1].item())  # synchronises the stream
         wall = time.perf_counter() - t0
@@ -321,7 +352,7 @@ class Simulator:
             "pcg_iter": pcg_it,
             "pcg_res": pcg_res,
             "max_div": div_after,
-            "droplets": 0,
+            "droplets": self._droplet_count() if self.cfg.droplets else 0,
             "wall_s": wall,
         }
         self.stats.append(rec)
@@ -418,10 +449,50 @@ class Simulator:
         self._g2p_advect(dt, do_g2p=False, do_advect=True)
 
     def _droplets(self, dt: float):
-        if self.cfg.droplets and not self._warned_droplets:
-            warnings.warn("the droplet/spray stage is not part of this implementation; cfg.droplets is ignored",
-                          RuntimeWarning, stacklevel=3)
-            self._warned_droplets = True
+        """Escaped particles -> droplets, droplet dynamics (pfflip/sim.py:343-392)."""
+        cfg = self.cfg
+        if not cfg.droplets or self.n_particles == 0:
+            return
+        mean_r = cfg.droplet_radius_mean * cfg.dx
+        sigma = float(cfg.droplet_radius_spread)
+        mu = float(np.log(mean_r) - 0.5 * sigma * sigma)  # pfflip/droplets.py:356-360
+        r_min, r_max = 0.02 * cfg.dx, 2.0 * cfg.dx
+        seed = (int(cfg.seed) + int(self.step_index)) & 0xFFFFFFFF
+        g, n, st = C.byref(self._g), self.n_particles, N.stream()
+        self._counters.zero_()
+        N.call("pf_droplet_classify", g, n, self._pos4.data_ptr(), self._vel4.data_ptr(), self._drop_r.data_ptr(),
+               N.ptr(self.phi_cell), float(cfg.delta_phi), mu, sigma, float(r_min), float(r_max), seed,
+               self._counters.data_ptr(), st)
+        if cfg.spray_shear_threshold > 0.0:
+            if self.shear is None:
+                self.shear = DeviceArray(torch.zeros(self.res, dtype=torch.float32, device=self.dev))
+            N.call("pf_velocity_gradient", g, *(N.ptr(a) for a in self.vel), N.ptr(self.shear), st)
+            N.call("pf_spray_emit", g, n, self._pos4.data_ptr(), self._vel4.data_ptr(), self._drop_r.data_ptr(),
+                   N.ptr(self.phi_cell), N.ptr(self.shear), float(cfg.spray_shear_threshold),
+                   float(cfg.spray_emission_rate), mu, sigma, float(r_min), float(r_max), seed,
+                   self._counters.data_ptr(), st)
+        lo, hi = self._bounds()
+        grav = (C.c_float * 3)(*[float(x) for x in cfg.gravity])
+        N.call("pf_droplet_advance", g, n, self._pos4.data_ptr(), self._vel4.data_ptr(), self._drop_r.data_ptr(),
+               *(N.ptr(a) for a in self.vel), float(dt), grav, float(cfg.rho_g), float(cfg.rho_l),
+               float(cfg.droplet_drag_cd), float(cfg.evaporation_k * cfg.dx * cfg.dx), float(r_min), lo, hi,
+               int(cfg.droplet_max_substeps), st)
+        c = self._counters.cpu().numpy()
+        for k, i in (("emitted", 0), ("bubbles", 1), ("merged", 2), ("spray", 3)):
+            self.droplet_stats[k] += int(c[i])
+
+    def _droplet_count(self) -> int:
+        return int((((self._flags() >> N_PSTATE_SHIFT) & 3) == 1).sum().item())
+
+    def rasterize_spray(self):
+        """Droplet volume splatted into the float16 spray density field at
+        spray_resolution_factor x the grid (pfflip/sim.py:394-401)."""
+        if self.spray_density is None:
+            self.spray_density = DeviceArray(torch.zeros(self.spray_res, dtype=torch.float16, device=self.dev))
+        sx, sy, sz = self.spray_res
+        N.call("pf_spray_rasterize", self.n_particles, self._pos4.data_ptr(), self._drop_r.data_ptr(),
+               N.ptr(self.spray_density), sx, sy, sz, float(self.dx_spray), N.stream())
+        return self.spray_density
 
     @property
     def dvel(self):

@@ -201,6 +201,54 @@ int pf_g2p_advect_packed(const pf_grid* g, int64_t n, float* pos4, float* vel4, 
  * replaces pfflip/kernels.py:552-564 (particle_max_speed). */
 int pf_particle_max_speed(int64_t n, const float* pos4, const float* vel4, float* out, void* stream);
 
+/* ------------------------------------------------------------- droplets */
+/* Escaped particles, droplets and spray; pfflip/droplets.py as run by
+ * pfflip/sim.py:343-401.  A particle's state is bits 1-2 of its flags
+ * (0 FLIP, 1 droplet, 2 dead); drop_r[n] is the droplet radius, in the order
+ * of pos4/vel4 (after a sort, permute it with pf_permute_f32 and perm_out).
+ * counters[4] accumulate (emitted, bubbles deleted, merged back, spray); the
+ * caller zeroes them.  Random numbers (radii, spray emission) come from a
+ * PCG-hash stream keyed by (seed, particle id = vel4.w), not from the
+ * reference's Warp stream: radii follow the same log-normal law
+ * exp(r_mu + r_sigma N(0,1)) clamped to [r_min, r_max], with other values. */
+
+/* classify_escaped (pfflip/droplets.py:67-106): liquid FLIP particles where
+ * the trilinear cell phi < 1/2 - delta_phi become droplets; air FLIP particles
+ * where phi > 1/2 + delta_phi die (bubbles); droplets where phi > 1/2 +
+ * delta_phi merge back. */
+int pf_droplet_classify(const pf_grid* g, int64_t n, float* pos4, const float* vel4, float* drop_r,
+                        const float* phi_cell, float delta_phi, float r_mu, float r_sigma, float r_min, float r_max,
+                        uint32_t seed, int32_t* counters, void* stream);
+
+/* velocity_gradient_magnitude (pfflip/droplets.py:153-194): |grad u| at cell
+ * centres from the MAC faces. */
+int pf_velocity_gradient(const pf_grid* g, const float* vel_x, const float* vel_y, const float* vel_z, float* out,
+                         void* stream);
+
+/* emit_spray_in_shear (pfflip/droplets.py:112-150): liquid FLIP particles of
+ * the interfacial band (0.1 <= phi <= 0.9) with shear >= threshold become
+ * droplets with probability rate. */
+int pf_spray_emit(const pf_grid* g, int64_t n, float* pos4, const float* vel4, float* drop_r, const float* phi_cell,
+                  const float* shear, float threshold, float rate, float r_mu, float r_sigma, float r_min, float r_max,
+                  uint32_t seed, int32_t* counters, void* stream);
+
+/* advance_droplets (pfflip/droplets.py:211-279): per-droplet sub-steps
+ * min(int(|v| dt / (dx/2)) + 1, max_substeps), gravity + sphere drag through
+ * the face velocities, evaporation dr/dt = -evap_k/r by RK2; droplets that
+ * leave [lo, hi] or shrink to r_min die. */
+int pf_droplet_advance(const pf_grid* g, int64_t n, float* pos4, float* vel4, float* drop_r, const float* vel_x,
+                       const float* vel_y, const float* vel_z, float dt, const float gravity[3], float rho_g,
+                       float rho_l, float drag_cd, float evap_k, float r_min, const float lo[3], const float hi[3],
+                       int32_t max_substeps, void* stream);
+
+/* rasterize_spray (pfflip/droplets.py:309-353): droplet volume splatted into
+ * a float16 grid (sx, sy, sz) of spacing dx_spray, zeroed first. */
+int pf_spray_rasterize(int64_t n, const float* pos4, const float* drop_r, void* density_f16, int32_t sx, int32_t sy,
+                       int32_t sz, float dx_spray, void* stream);
+
+/* out[t] = in[perm[t]]: a per-particle float follows the sort. */
+int pf_permute_f32(int64_t n, const int32_t* perm, const float* in, float* out, void* stream);
+
 /* --------------------------------------------------------------- Poisson */
 /* (Ap)_i = sum_f beta_f (p_i - p_nbr) with clamped neighbour indices;
  * replaces pfflip/poisson.py:54-88 (apply_A).  stencil = PF_STENCIL_REFERENCE

@@ -64,6 +64,13 @@ def lib():
             g("g2p").argtypes = [I64, fp, fp, i32p, i32p] + [fp] * 6 + [I, I, I, R, R, R]
             g("advect_reflect").argtypes = [I64, fp, fp, i32p, i32p] + [fp] * 6 + [I, I, I, R, R, fp, fp]
             g("push_out_of_solids").argtypes = [I64, fp, fp, i32p, i32p, I, I, I, R]
+            U32 = C.c_uint32
+            g("droplet_classify").argtypes = [I64, fp, i32p, i32p, fp, fp, I, I, I, R, R, R, R, R, R, U32, i32p]
+            g("velocity_gradient").argtypes = [fp, fp, fp, fp, I, I, I, R]
+            g("spray_emit").argtypes = [I64, fp, i32p, i32p, fp, fp, fp, I, I, I, R, R, R, R, R, R, R, U32, i32p]
+            g("droplet_advance").argtypes = [I64, fp, fp, i32p, fp, fp, fp, fp, I, I, I, R, R, fp, R, R, R, R, R,
+                                             fp, fp, I]
+            g("spray_rasterize").argtypes = [I64, fp, i32p, fp, fp, I, I, I, R]
             g("particle_max_speed").argtypes = [I64, fp, i32p]
             g("particle_max_speed").restype = R
             g("apply_A").argtypes = [fp] * 6 + [I, I, I]
@@ -286,6 +293,10 @@ class OracleSim:
         self.step_index = 0
         self.stats = []
         self.n_particles = 0
+        self.droplet_stats = {"emitted": 0, "bubbles": 0, "merged": 0, "spray": 0}
+        f = max(1, int(cfg.spray_resolution_factor))
+        self.spray_res = tuple(n * f for n in self.res)
+        self.dx_spray = cfg.dx / f
 
     def _c(self, x):
         return self.R.type(x)
@@ -304,6 +315,7 @@ class OracleSim:
         self.pmass = np.where(self.ptype == 1, cfg.rho_l, cfg.rho_g).astype(R)
         self.prad = np.full(n, cfg.r_p, R)
         self.pstate = np.zeros(n, np.int32) if pstate is None else np.ascontiguousarray(pstate, np.int32).copy()
+        self.pdrop_r = np.zeros(n, R)
 
     # ----------------------------------------------------------- stages
     def _p2g(self):
@@ -399,6 +411,43 @@ class OracleSim:
             _fn("push_out_of_solids", self.R)(self.n_particles, self.px, self.pv, self.pstate, self.solid,
                                               *self.res, self._c(cfg.dx))
 
+    def _droplets(self, dt):
+        """``pfflip/sim.py:343-392``: classification, optional shear spray, droplet dynamics."""
+        cfg, c, R = self.cfg, self._c, self.R
+        if not cfg.droplets or self.n_particles == 0:
+            return
+        sigma = float(cfg.droplet_radius_spread)
+        mu = float(np.log(cfg.droplet_radius_mean * cfg.dx) - 0.5 * sigma * sigma)
+        r_min, r_max = 0.02 * cfg.dx, 2.0 * cfg.dx
+        seed = (int(cfg.seed) + int(self.step_index)) & 0xFFFFFFFF
+        counters = np.zeros(4, np.int32)
+        nx, ny, nz = self.res
+        _fn("droplet_classify", R)(self.n_particles, self.px, self.ptype, self.pstate, self.pdrop_r, self.phi_cell,
+                                   nx, ny, nz, c(cfg.dx), c(cfg.delta_phi), c(mu), c(sigma), c(r_min), c(r_max),
+                                   seed, counters)
+        if cfg.spray_shear_threshold > 0.0:
+            self.shear = np.zeros(self.res, R)
+            _fn("velocity_gradient", R)(*self.vel, self.shear, nx, ny, nz, c(cfg.dx))
+            _fn("spray_emit", R)(self.n_particles, self.px, self.ptype, self.pstate, self.pdrop_r, self.phi_cell,
+                                 self.shear, nx, ny, nz, c(cfg.dx), c(cfg.spray_shear_threshold),
+                                 c(cfg.spray_emission_rate), c(mu), c(sigma), c(r_min), c(r_max), seed, counters)
+        eps = 1e-4 * cfg.dx
+        lo = np.full(3, eps, R)
+        hi = np.array([s - eps for s in cfg.domain_size], R)
+        _fn("droplet_advance", R)(self.n_particles, self.px, self.pv, self.pstate, self.pdrop_r, *self.vel, nx, ny,
+                                  nz, c(dt), c(cfg.dx), np.asarray(cfg.gravity, R), c(cfg.rho_g), c(cfg.rho_l),
+                                  c(cfg.droplet_drag_cd), c(cfg.evaporation_k * cfg.dx * cfg.dx), c(r_min), lo, hi,
+                                  int(cfg.droplet_max_substeps))
+        for k, i in (("emitted", 0), ("bubbles", 1), ("merged", 2), ("spray", 3)):
+            self.droplet_stats[k] += int(counters[i])
+
+    def rasterize_spray(self):
+        """``pfflip/sim.py:394-401`` (accumulated in the oracle's precision)."""
+        out = np.zeros(self.spray_res, self.R)
+        _fn("spray_rasterize", self.R)(self.n_particles, self.px, self.pstate, self.pdrop_r, out, *self.spray_res,
+                                       self._c(self.dx_spray))
+        return out
+
     def dt_from_cfl(self):
         cfg = self.cfg
         vmax = float(_fn("particle_max_speed", self.R)(self.n_particles, self.pv, self.pstate))
@@ -418,10 +467,11 @@ class OracleSim:
         div = self._max_divergence()
         self._g2p()
         self._extrapolate_liquid_velocity()
+        self._droplets(dt)
         self._advect(dt)
         self.time += dt
         self.step_index += 1
         rec = {"step": self.step_index, "t": self.time, "dt": dt, "pcg_iter": it, "pcg_res": rel,
-               "max_div": div, "droplets": 0}
+               "max_div": div, "droplets": int((self.pstate == 1).sum()) if self.cfg.droplets else 0}
         self.stats.append(rec)
         return rec

@@ -88,6 +88,32 @@ void pfo_sort_by_cell(int64_t n, const float* pos, float dx, int nx, int ny, int
                                     int nx, int ny, int nz, R dx) {                                               \
     push_out_of_solids(n, px, pv, pstate, solid, nx, ny, nz, dx);                                                 \
   }                                                                                                               \
+  void pfo_droplet_classify_##SFX(int64_t n, const R* px, const int32_t* ptype, int32_t* pstate, R* pdrop_r,     \
+                                  const R* phi, int nx, int ny, int nz, R dx, R delta_phi, R mu, R sigma, R rmin, \
+                                  R rmax, uint32_t seed, int32_t* counters) {                                     \
+    droplet_classify(n, px, ptype, pstate, pdrop_r, phi, nx, ny, nz, dx, delta_phi, mu, sigma, rmin, rmax, seed,  \
+                     counters);                                                                                   \
+  }                                                                                                               \
+  void pfo_velocity_gradient_##SFX(const R* u, const R* v, const R* w, R* out, int nx, int ny, int nz, R dx) {    \
+    velocity_gradient(u, v, w, out, nx, ny, nz, dx);                                                              \
+  }                                                                                                               \
+  void pfo_spray_emit_##SFX(int64_t n, const R* px, const int32_t* ptype, int32_t* pstate, R* pdrop_r,            \
+                            const R* phi, const R* shear, int nx, int ny, int nz, R dx, R threshold, R rate,      \
+                            R mu, R sigma, R rmin, R rmax, uint32_t seed, int32_t* counters) {                    \
+    spray_emit(n, px, ptype, pstate, pdrop_r, phi, shear, nx, ny, nz, dx, threshold, rate, mu, sigma, rmin, rmax, \
+               seed, counters);                                                                                   \
+  }                                                                                                               \
+  void pfo_droplet_advance_##SFX(int64_t n, R* px, R* pv, int32_t* pstate, R* pdrop_r, const R* u0, const R* u1,  \
+                                 const R* u2, int nx, int ny, int nz, R dt, R dx, const R* grav, R rho_g,         \
+                                 R rho_l, R cd, R evap_k, R rmin, const R* lo, const R* hi, int max_sub) {        \
+    const R* u[3] = {u0, u1, u2};                                                                                 \
+    droplet_advance(n, px, pv, pstate, pdrop_r, u, nx, ny, nz, dt, dx, grav, rho_g, rho_l, cd, evap_k, rmin, lo,  \
+                    hi, max_sub);                                                                                 \
+  }                                                                                                               \
+  void pfo_spray_rasterize_##SFX(int64_t n, const R* px, const int32_t* pstate, const R* pdrop_r, R* density,     \
+                                 int sx, int sy, int sz, R dxs) {                                                 \
+    spray_rasterize(n, px, pstate, pdrop_r, density, sx, sy, sz, dxs);                                            \
+  }                                                                                                               \
   R pfo_particle_max_speed_##SFX(int64_t n, const R* pv, const int32_t* pstate) {                                 \
     return particle_max_speed(n, pv, pstate);                                                                     \
   }                                                                                                               \

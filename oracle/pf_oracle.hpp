@@ -522,6 +522,209 @@ template <class R> inline R particle_max_speed(int64_t n, const R* pv, const int
 }
 
 // ===========================================================================
+// Droplets: pfflip/droplets.py (escaped particles, droplet dynamics, spray)
+// ===========================================================================
+// The reference draws radii and spray emission from Warp's rand stream, which
+// is not available here.  The library and this oracle share a documented
+// stream instead: the PCG-RXS-M-XS 32-bit hash, seeded per particle id with
+// hash(hash(seed) + id), uniforms ((s >> 8) + 0.5) * 2^-24, normals by
+// Box-Muller, all in binary32.
+inline uint32_t pcg_hash(uint32_t v) {
+  const uint32_t s = v * 747796405u + 2891336453u;
+  const uint32_t w = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
+  return (w >> 22u) ^ w;
+}
+struct DropRng {
+  uint32_t s;
+  DropRng(uint32_t seed, uint32_t id) : s(pcg_hash(pcg_hash(seed) + id)) {}
+  float uniform() {
+    s = pcg_hash(s);
+    return ((float)(s >> 8) + 0.5f) * (1.0f / 16777216.0f);
+  }
+  float normal() {
+    const float u1 = uniform(), u2 = uniform();
+    return std::sqrt(-2.0f * std::log(u1)) * std::cos(6.28318530717958647692f * u2);
+  }
+};
+
+// pfflip/droplets.py:41-64 sample_cell
+template <class R> inline R sample_cell(const R* f, Dims d, const R x[3], R dx) {
+  R g0 = x[0] / dx - R(0.5), g1 = x[1] / dx - R(0.5), g2 = x[2] / dx - R(0.5);
+  int i0 = (int)std::floor(g0), j0 = (int)std::floor(g1), k0 = (int)std::floor(g2);
+  R tx = g0 - (R)i0, ty = g1 - (R)j0, tz = g2 - (R)k0;
+  R acc = R(0);
+  for (int a = 0; a < 2; ++a) {
+    R wa = a == 0 ? R(1) - tx : tx;
+    int ii = std::min(std::max(i0 + a, 0), d.n0 - 1);
+    for (int b = 0; b < 2; ++b) {
+      R wb = b == 0 ? R(1) - ty : ty;
+      int jj = std::min(std::max(j0 + b, 0), d.n1 - 1);
+      for (int c = 0; c < 2; ++c) {
+        R wc = c == 0 ? R(1) - tz : tz;
+        int kk = std::min(std::max(k0 + c, 0), d.n2 - 1);
+        acc += wa * wb * wc * f[d.at(ii, jj, kk)];
+      }
+    }
+  }
+  return acc;
+}
+
+// pfflip/droplets.py:67-106 classify_escaped (counters: emitted, bubbles, merged, spray)
+template <class R>
+inline void droplet_classify(int64_t n, const R* px, const int32_t* ptype, int32_t* pstate, R* pdrop_r,
+                             const R* phi, int nx, int ny, int nz, R dx, R delta_phi, R mu, R sigma, R rmin,
+                             R rmax, uint32_t seed, int32_t* counters) {
+  Dims cd{nx, ny, nz};
+  for (int64_t p = 0; p < n; ++p) {
+    const int st = pstate[p];
+    if (st == 2) continue;
+    const R f = sample_cell(phi, cd, px + 3 * p, dx);
+    if (st == 0) {
+      if (ptype[p] == 1 && f < R(0.5) - delta_phi) {
+        pstate[p] = 1;
+        DropRng rng(seed, (uint32_t)p);
+        const R r = std::exp(mu + sigma * (R)rng.normal());
+        pdrop_r[p] = std::min(std::max(r, rmin), rmax);
+        counters[0] += 1;
+      } else if (ptype[p] == 0 && f > R(0.5) + delta_phi) {
+        pstate[p] = 2;
+        counters[1] += 1;
+      }
+    } else if (st == 1 && f > R(0.5) + delta_phi) {
+      pstate[p] = 0;
+      counters[2] += 1;
+    }
+  }
+}
+
+// pfflip/droplets.py:153-194 velocity_gradient_magnitude
+template <class R>
+inline void velocity_gradient(const R* u, const R* v, const R* w, R* out, int nx, int ny, int nz, R dx) {
+  Dims fu = face_dims(nx, ny, nz, 0), fv = face_dims(nx, ny, nz, 1), fw = face_dims(nx, ny, nz, 2), cd{nx, ny, nz};
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        R dudx = (u[fu.at(i + 1, j, k)] - u[fu.at(i, j, k)]) / dx;
+        R dvdy = (v[fv.at(i, j + 1, k)] - v[fv.at(i, j, k)]) / dx;
+        R dwdz = (w[fw.at(i, j, k + 1)] - w[fw.at(i, j, k)]) / dx;
+        R acc = dudx * dudx + dvdy * dvdy + dwdz * dwdz;
+        int jm = std::max(j - 1, 0), jp = std::min(j + 1, ny - 1), km = std::max(k - 1, 0),
+            kp = std::min(k + 1, nz - 1), im = std::max(i - 1, 0), ip = std::min(i + 1, nx - 1);
+        R dudy = (R(0.5) * (u[fu.at(i, jp, k)] + u[fu.at(i + 1, jp, k)]) -
+                  R(0.5) * (u[fu.at(i, jm, k)] + u[fu.at(i + 1, jm, k)])) / (R(2) * dx);
+        R dudz = (R(0.5) * (u[fu.at(i, j, kp)] + u[fu.at(i + 1, j, kp)]) -
+                  R(0.5) * (u[fu.at(i, j, km)] + u[fu.at(i + 1, j, km)])) / (R(2) * dx);
+        R dvdx = (R(0.5) * (v[fv.at(ip, j, k)] + v[fv.at(ip, j + 1, k)]) -
+                  R(0.5) * (v[fv.at(im, j, k)] + v[fv.at(im, j + 1, k)])) / (R(2) * dx);
+        R dwdx = (R(0.5) * (w[fw.at(ip, j, k)] + w[fw.at(ip, j, k + 1)]) -
+                  R(0.5) * (w[fw.at(im, j, k)] + w[fw.at(im, j, k + 1)])) / (R(2) * dx);
+        acc += dudy * dudy + dudz * dudz + dvdx * dvdx + dwdx * dwdx;
+        out[cd.at(i, j, k)] = std::sqrt(acc);
+      }
+}
+
+// pfflip/droplets.py:112-150 emit_spray_in_shear
+template <class R>
+inline void spray_emit(int64_t n, const R* px, const int32_t* ptype, int32_t* pstate, R* pdrop_r, const R* phi,
+                       const R* shear, int nx, int ny, int nz, R dx, R threshold, R rate, R mu, R sigma, R rmin,
+                       R rmax, uint32_t seed, int32_t* counters) {
+  Dims cd{nx, ny, nz};
+  for (int64_t p = 0; p < n; ++p) {
+    if (pstate[p] != 0 || ptype[p] != 1) continue;
+    const R f = sample_cell(phi, cd, px + 3 * p, dx);
+    if (f > R(0.9) || f < R(0.1)) continue;
+    if (sample_cell(shear, cd, px + 3 * p, dx) < threshold) continue;
+    DropRng rng(seed + 104729u, (uint32_t)p);
+    if ((R)rng.uniform() > rate) continue;
+    pstate[p] = 1;
+    pdrop_r[p] = std::min(std::max((R)std::exp(mu + sigma * (R)rng.normal()), rmin), rmax);
+    counters[3] += 1;
+  }
+}
+
+// pfflip/droplets.py:197-279 drag_acceleration + advance_droplets
+template <class R>
+inline void droplet_advance(int64_t n, R* px, R* pv, int32_t* pstate, R* pdrop_r, const R* u[3], int nx, int ny,
+                            int nz, R dt, R dx, const R grav[3], R rho_g, R rho_l, R cd, R evap_k, R rmin,
+                            const R lo[3], const R hi[3], int max_sub) {
+  Dims fd[3] = {face_dims(nx, ny, nz, 0), face_dims(nx, ny, nz, 1), face_dims(nx, ny, nz, 2)};
+  for (int64_t p = 0; p < n; ++p) {
+    if (pstate[p] != 1) continue;
+    R x[3] = {px[3 * p], px[3 * p + 1], px[3 * p + 2]}, v[3] = {pv[3 * p], pv[3 * p + 1], pv[3 * p + 2]};
+    R r = pdrop_r[p];
+    const R speed = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) + R(1e-8);
+    const int nsub = std::min(std::max((int)(speed * dt / (R(0.5) * dx)) + 1, 1), max_sub);
+    const R h = dt / (R)nsub;
+    bool dead = false;
+    for (int s = 0; s < nsub && !dead; ++s) {
+      R ua[3];
+      for (int c = 0; c < 3; ++c) ua[c] = sample_face(u[c], fd[c], x, dx, c);
+      R vr[3] = {ua[0] - v[0], ua[1] - v[1], ua[2] - v[2]};
+      R sr = std::sqrt(vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]);
+      bool drag = sr > R(0) && r > R(0);
+      R coef = drag ? (R(3) * rho_g * cd * sr / (R(8) * rho_l * r)) : R(0);
+      for (int c = 0; c < 3; ++c) {
+        R acc = grav[c] + (drag ? coef * vr[c] : R(0));
+        v[c] = v[c] + h * acc;
+        x[c] = x[c] + h * v[c];
+      }
+      if (evap_k > R(0) && r > R(0)) {
+        R k1 = -evap_k / r;
+        R rm = std::max(r + R(0.5) * h * k1, R(1e-9));
+        r = r + h * (-evap_k / rm);
+        if (r <= rmin) dead = true;
+      }
+    }
+    if (!dead)
+      for (int c = 0; c < 3; ++c)
+        if (x[c] <= lo[c] || x[c] >= hi[c]) dead = true;
+    if (dead) {
+      pstate[p] = 2;
+      continue;
+    }
+    pdrop_r[p] = r;
+    for (int c = 0; c < 3; ++c) {
+      pv[3 * p + c] = v[c];
+      px[3 * p + c] = x[c];
+    }
+  }
+}
+
+// pfflip/droplets.py:309-353 rasterize_spray (accumulated in R here; the
+// reference and the library add float16 values)
+template <class R>
+inline void spray_rasterize(int64_t n, const R* px, const int32_t* pstate, const R* pdrop_r, R* density, int sx,
+                            int sy, int sz, R dxs) {
+  Dims d{sx, sy, sz};
+  std::fill(density, density + d.size(), R(0));
+  for (int64_t p = 0; p < n; ++p) {
+    if (pstate[p] != 1) continue;
+    const R r = pdrop_r[p];
+    const R vol = R(4.0 / 3.0) * R(3.14159265) * r * r * r;
+    R g0 = px[3 * p] / dxs - R(0.5), g1 = px[3 * p + 1] / dxs - R(0.5), g2 = px[3 * p + 2] / dxs - R(0.5);
+    int i0 = (int)std::floor(g0), j0 = (int)std::floor(g1), k0 = (int)std::floor(g2);
+    R tx = g0 - (R)i0, ty = g1 - (R)j0, tz = g2 - (R)k0;
+    const R cv = dxs * dxs * dxs;
+    for (int a = 0; a < 2; ++a) {
+      R wa = a == 0 ? R(1) - tx : tx;
+      int ii = i0 + a;
+      if (ii < 0 || ii >= sx) continue;
+      for (int b = 0; b < 2; ++b) {
+        R wb = b == 0 ? R(1) - ty : ty;
+        int jj = j0 + b;
+        if (jj < 0 || jj >= sy) continue;
+        for (int c = 0; c < 2; ++c) {
+          R wc = c == 0 ? R(1) - tz : tz;
+          int kk = k0 + c;
+          if (kk < 0 || kk >= sz) continue;
+          density[d.at(ii, jj, kk)] += wa * wb * wc * vol / cv;
+        }
+      }
+    }
+  }
+}
+
+// ===========================================================================
 // Poisson: pfflip/poisson.py
 // ===========================================================================
 template <class R> struct Level {

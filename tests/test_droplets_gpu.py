@@ -1,0 +1,152 @@
+"""The droplet stage (pf_droplet_*, pf_spray_*) against the CPU oracle.
+
+The stage is compared from one snapshot of the GPU state, so both sides start
+from the same particles, phase field and velocities:
+
+* states and counters: equal, except for particles whose sampled phi lies
+  within rounding of a threshold (FMA contraction differs), at most
+  max(2, 1e-5 n) of them;
+* radii: the library and the oracle share a documented random stream keyed by
+  particle id, so radii agree to 1e-5 relative (expf/logf/cosf rounding);
+* droplet positions and velocities after the sub-stepped dynamics: 1e-5
+  relative to the largest value;
+* the float16 spray raster: 1e-2 of its maximum (float16 adds vs binary32).
+The radius law itself (log-normal with the configured mean) is checked on
+the GPU stream.
+"""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from pfflip import Config, Simulator, scenes
+from pfflip import _native as N
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+
+
+def snapshot(steps=6, spray=0.0):
+    cfg = Config(res=(32,) * 3, dx=1 / 32, cfl=1.0, device=DEV, ppc=27, droplets=True,
+                 spray_shear_threshold=spray, spray_emission_rate=0.5)
+    sim = Simulator(cfg)
+    sim.set_particles(*scenes.asteroid_impact(cfg))
+    for _ in range(steps):
+        sim.step()
+    o = O.OracleSim(cfg, stencil=cfg.stencil)
+    o.set_particles(sim.px.numpy(), sim.pv.numpy(), sim.ptype.numpy(), pstate=sim.pstate.numpy())
+    o.pdrop_r[...] = sim.pdrop_r.numpy()
+    o.phi_cell[...] = sim.phi_cell.numpy()
+    for ax in range(3):
+        o.vel[ax][...] = sim.vel[ax].numpy()
+    o.step_index = sim.step_index
+    return cfg, sim, o
+
+
+def compare_stage(sim, o, dt):
+    n = sim.n_particles
+    before = dict(sim.droplet_stats)  # the GPU stats count the snapshot's own steps too
+    sim._droplets(dt)
+    o._droplets(dt)
+    st_g, st_o = sim.pstate.numpy(), o.pstate
+    bad = st_g != st_o
+    assert bad.sum() <= max(2, int(1e-5 * n)), int(bad.sum())
+    for k in ("emitted", "bubbles", "merged", "spray"):
+        d = sim.droplet_stats[k] - before[k]
+        assert abs(d - o.droplet_stats[k]) <= bad.sum(), (k, d, o.droplet_stats)
+    drop = (st_g == 1) & ~bad
+    r_g, r_o = sim.pdrop_r.numpy()[drop], o.pdrop_r[drop]
+    assert np.abs(r_g - r_o).max() <= 1e-5 * np.abs(r_o).max()
+    for a, b in ((sim.px.numpy()[drop], o.px[drop]), (sim.pv.numpy()[drop], o.pv[drop])):
+        assert np.abs(a - b).max() <= 1e-5 * max(np.abs(b).max(), 1.0)
+    return int(drop.sum())
+
+
+def test_droplet_stage_matches_oracle():
+    cfg, sim, o = snapshot()
+    dt = 0.5 * cfg.dx / 4.0
+    ndrop = compare_stage(sim, o, dt)
+    assert ndrop > 0 and sim.droplet_stats["emitted"] > 0
+
+
+def test_shear_spray_matches_oracle():
+    cfg, sim, o = snapshot(spray=1e-30)  # any threshold > 0 switches the channel on
+    # threshold at the median shear of the interfacial band, so part of the band qualifies
+    shear = torch.zeros(cfg.res, device=DEV)
+    g = C.byref(sim._g)
+    N.call("pf_velocity_gradient", g, *(N.ptr(a) for a in sim.vel), shear.data_ptr(), N.stream())
+    ref = np.zeros(cfg.res, np.float32)
+    O._fn("velocity_gradient", np.float32)(*o.vel, ref, *cfg.res, np.float32(cfg.dx))
+    assert np.abs(shear.cpu().numpy() - ref).max() <= 1e-5 * np.abs(ref).max()
+    thr = float(np.median(ref[ref > 0]))
+    sim.cfg.spray_shear_threshold = thr
+    o.cfg.spray_shear_threshold = thr
+    before = sim.droplet_stats["spray"]
+    compare_stage(sim, o, 0.5 * cfg.dx / 4.0)
+    assert sim.droplet_stats["spray"] > before
+
+
+def test_spray_raster_matches_oracle():
+    cfg, sim, o = snapshot()
+    compare_stage(sim, o, 0.5 * cfg.dx / 4.0)  # fresh droplets on both sides
+    assert (sim.pstate.numpy() == 1).sum() > 0
+    dens = sim.rasterize_spray().numpy().astype(np.float32)
+    ref = o.rasterize_spray()
+    assert ref.max() > 0
+    assert np.abs(dens - ref).max() <= 1e-2 * ref.max() + 1e-3
+
+
+def test_radius_law_is_lognormal_with_configured_mean():
+    """All-liquid particles in phi = 0 all convert; their radii follow
+    exp(mu + sigma N(0,1)) with mean radius droplet_radius_mean * dx."""
+    res = (16, 16, 16)
+    dx = 1 / 16
+    g = N.grid(res, np.float32(dx))
+    n = 200_000
+    rng = np.random.default_rng(3)
+    p4 = torch.zeros((n, 4), device=DEV)
+    p4[:, :3] = torch.tensor(rng.random((n, 3)).astype(np.float32), device=DEV)
+    p4.view(torch.int32)[:, 3] = 1  # liquid, FLIP
+    v4 = torch.zeros((n, 4), device=DEV)
+    v4.view(torch.int32)[:, 3] = torch.arange(n, dtype=torch.int32, device=DEV)
+    r = torch.zeros(n, device=DEV)
+    phi = torch.zeros(res, device=DEV)
+    cnt = torch.zeros(4, dtype=torch.int32, device=DEV)
+    mean_r, sigma = 0.25 * dx, 0.5
+    mu = float(np.log(mean_r) - 0.5 * sigma * sigma)
+    N.call("pf_droplet_classify", C.byref(g), n, p4.data_ptr(), v4.data_ptr(), r.data_ptr(), phi.data_ptr(), 0.2, mu,
+           sigma, 0.0, 1.0, 7, cnt.data_ptr(), N.stream())
+    assert int(cnt[0]) == n
+    rr = r.cpu().numpy().astype(np.float64)
+    assert abs(rr.mean() / mean_r - 1) < 0.01
+    assert abs(np.log(rr).std() / sigma - 1) < 0.01
+    assert abs(np.log(rr).mean() - mu) < 0.01 * sigma
+    # the stream is keyed by particle id: a second call draws the same radii
+    p4.view(torch.int32)[:, 3] = 1
+    r2 = torch.zeros(n, device=DEV)
+    N.call("pf_droplet_classify", C.byref(g), n, p4.data_ptr(), v4.data_ptr(), r2.data_ptr(), phi.data_ptr(), 0.2,
+           mu, sigma, 0.0, 1.0, 7, cnt.data_ptr(), N.stream())
+    assert torch.equal(r, r2)
+
+
+def test_full_steps_with_droplets_match_oracle():
+    """Two whole steps with the droplet stage on, GPU vs oracle from the same
+    particles: the same transitions, and particles of equal state stay close."""
+    cfg = Config(res=(16,) * 3, dx=1 / 16, device=DEV, ppc=27, droplets=True, pcg_tol=1e-6, seed=5)
+    pos, vel, pt = scenes.asteroid_impact(cfg)
+    dt = 0.25 * cfg.dx / 4.0
+    sim = Simulator(cfg)
+    sim.set_particles(pos, vel, pt)
+    o = O.OracleSim(cfg, stencil=cfg.stencil)
+    o.set_particles(pos, vel, pt)
+    for _ in range(2):
+        sim.step(dt)
+        o.step(dt)
+    st_g, st_o = sim.pstate.numpy(), o.pstate
+    bad = st_g != st_o
+    assert bad.sum() <= max(2, int(1e-4 * len(pos)))
+    ok = ~bad & (st_g != 2)
+    assert np.abs(sim.px.numpy()[ok] - o.px[ok]).max() < 1e-3 * cfg.dx

@@ -1,12 +1,8 @@
 """The reference's end-to-end property tests (tests/test_pfflip.py) run against
 the drop-in Simulator on the GPU.
 
-Same scenes, sizes, step counts and thresholds as the reference file
-(line numbers in each docstring).  The droplet stage is outside this
-implementation, so configurations set ``droplets=False`` and the two
-droplet-transition tests of the reference (:124-137, :140-167 asserts on
-droplet conversion) are not ported; the ones that only use ``pstate``
-(:170-189, :245-268) are.
+Same scenes, sizes, step counts, droplet settings and thresholds as the
+reference file (line numbers in each docstring).
 """
 
 import math
@@ -108,10 +104,24 @@ def test_projection_reduces_divergence(stencil):
     assert div_after < 0.05 * div_before, f"{div_before:.3e} -> {div_after:.3e}"
 
 
+def test_bubbles_are_deleted_and_droplets_merge_back():
+    """tests/test_pfflip.py:124-137: the escaped-particle transitions fire."""
+    cfg = Config(res=(32,) * 3, dx=1 / 32, cfl=1.0, device=DEV, ppc=27, droplets=True, delta_phi=0.2)
+    sim = Simulator(cfg)
+    sim.set_particles(*scenes.asteroid_impact(cfg))
+    for _ in range(25):
+        sim.step()
+    s = sim.droplet_stats
+    assert s["bubbles"] > 0, "air particles trapped in liquid are never deleted"
+    counts = sim.state_counts()
+    assert counts["flip"] + counts["droplet"] + counts["dead"] == sim.n_particles
+    assert counts["dead"] == s["bubbles"] or counts["dead"] >= s["bubbles"] - s["merged"]
+
+
 def test_droplet_threshold_is_coupled_to_particle_count():
-    """tests/test_pfflip.py:140-167, its rho~_0 part (no droplet stage here)."""
+    """tests/test_pfflip.py:140-167"""
     for ppc in (8, 27):
-        cfg = Config(res=(16,) * 3, dx=1 / 16, device=DEV, ppc=ppc, droplets=False)
+        cfg = Config(res=(16,) * 3, dx=1 / 16, device=DEV, ppc=ppc)
         sim = Simulator(cfg)
         phi_single = 1.0 / math.sqrt(cfg.alpha_phi * sim.rho_tilde_0)
         predicted = 0.638 * ppc
@@ -121,7 +131,7 @@ def test_droplet_threshold_is_coupled_to_particle_count():
 
 def test_droplets_do_not_contribute_to_the_grid():
     """tests/test_pfflip.py:170-189: particles with pstate != 0 do not splat."""
-    cfg = Config(res=(16,) * 3, dx=1 / 16, cfl=1.0, device=DEV, ppc=8, droplets=False)
+    cfg = Config(res=(16,) * 3, dx=1 / 16, cfl=1.0, device=DEV, ppc=8, droplets=True)
     sim = Simulator(cfg)
     sim.set_particles(*scenes.still_pool(cfg, fill=0.5))
     sim.step()
@@ -174,7 +184,7 @@ def test_obstacle_scene_stays_bounded():
 
 def test_droplets_do_not_throttle_the_time_step():
     """tests/test_pfflip.py:245-268"""
-    cfg = Config(res=(32,) * 3, dx=1 / 32, cfl=1.0, device=DEV, ppc=8, droplets=False)
+    cfg = Config(res=(32,) * 3, dx=1 / 32, cfl=1.0, device=DEV, ppc=8, droplets=True)
     sim = Simulator(cfg)
     sim.set_particles(*scenes.asteroid_impact(cfg))
     sim.step()
