@@ -76,6 +76,10 @@ def parse():
     ap.add_argument("--adjoint-steps", type=int, default=20)
     ap.add_argument("--adjoint-fd", action="store_true",
                     help="check the gradient against FP64 central differences of the CPU oracle (slow)")
+    ap.add_argument("--rt", action="store_true",
+                    help="also time the Rayleigh-Taylor workload (256^3, 8 ppc, 16 modes), FP32 and 16-bit hierarchy")
+    ap.add_argument("--rt-only", action="store_true", help="only the Rayleigh-Taylor leg (prints its JSON)")
+    ap.add_argument("--rt-res", type=int, default=256)
     ap.add_argument("--adjoint-fd-res", type=int, default=None,
                     help="grid of the finite-difference check (default: --adjoint-res)")
     return ap.parse_args()
@@ -368,6 +372,11 @@ def run_ours(args):
         torch.cuda.empty_cache()
         line["adjoint"] = adjoint_leg(args)
 
+    if args.rt and rank == 0:
+        sim = None
+        torch.cuda.empty_cache()
+        line["rayleigh_taylor"] = rt_leg(args)
+
     # CPU baseline: the oracle on a bounded sample of the same workload
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         threads = os.cpu_count() or 1
@@ -449,6 +458,45 @@ def mixed_leg(args, pos, vel, pt, dt, ms_fp32):
         del sim
         torch.cuda.empty_cache()
     return res
+
+
+def rt_leg(args):
+    """Rayleigh-Taylor: heavy phase (1000) over light (1) across
+    y = 0.5 + sum_k a_k cos(2 pi (m_k x + n_k z)), 16 modes with a_k ~ U(0, 0.01)
+    and (m_k, n_k) in 1..4 drawn from the seed; 8 ppc.  Steps/s of the plain
+    FP32 step and of the 16-bit-hierarchy step at the same fixed dt."""
+    import torch
+
+    from pfflip import Config, Simulator, scenes
+
+    r = args.rt_res
+    base = Config(res=(r, r, r), dx=1.0 / r, ppc=8, seed=42, droplets=False, pcg_tol=args.tol, device="cuda")
+    t0 = time.perf_counter()
+    pos, vel, pt, amps, waves = scenes.rayleigh_taylor_modes(base)
+    seed_s = time.perf_counter() - t0
+    dt = fixed_dt(base.dx)
+    out = {"workload": f"rayleigh_taylor {r}^3 8ppc 16 modes", "particles": int(len(pos)), "dt": dt,
+           "seed_s": seed_s, "modes": {"a": [float(a) for a in amps], "mn": [[int(m), int(n)] for m, n in waves]}}
+    for prec in ("fp32", "fp16"):
+        cfg = Config(res=(r, r, r), dx=1.0 / r, ppc=8, seed=42, droplets=False, pcg_tol=args.tol, device="cuda",
+                     precision=prec)
+        sim = Simulator(cfg)
+        sim.set_particles(pos, vel, pt)
+        for _ in range(2):
+            sim.step(dt)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        recs = [sim.step(dt) for _ in range(max(args.steps // 2, 3))]
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / len(recs)
+        out[prec] = {"ms_per_step": ms, "steps_per_s": 1000.0 / ms,
+                     "pcg_iter_mean": float(np.mean([x["pcg_iter"] for x in recs])),
+                     "max_div": float(recs[-1]["max_div"])}
+        del sim
+        torch.cuda.empty_cache()
+    return out
 
 
 def adjoint_leg(args):
@@ -551,6 +599,12 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.rt_only:
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps({"rayleigh_taylor": rt_leg(args)}), flush=True)
+        return 0
     if args.adjoint_only:
         import torch
 

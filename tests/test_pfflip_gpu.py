@@ -216,3 +216,26 @@ def test_particle_views_round_trip():
     assert np.array_equal(sim.px.numpy(), pos2) and np.array_equal(sim.pv.numpy(), vel)
     assert sim.pmass.numpy().dtype == np.float32
     assert sim.state_counts() == {"flip": len(pos), "droplet": 0, "dead": 0}
+
+
+def test_save_frame_writes_the_reference_format(tmp_path):
+    """pfflip/io.py:10-29: keys, dtypes, strided particles in the caller's order."""
+    from pfflip import io
+
+    cfg = Config(res=(16,) * 3, dx=1 / 16, device=DEV, ppc=8, droplets=False)
+    sim = Simulator(cfg)
+    pos, vel, pt = scenes.dam_break(cfg)
+    sim.set_particles(pos, vel, pt)
+    sim.step()
+    path = str(tmp_path / "frames" / "frame_0001.npz")
+    io.save_frame(sim, path, stride=3)
+    f = io.load_frame(path)
+    assert set(f) == {"t", "step", "dx", "phi", "px", "ptype"}
+    assert f["t"].dtype == np.float32 and f["step"].dtype == np.int32 and f["dx"].dtype == np.float32
+    assert f["phi"].dtype == np.float16 and f["px"].dtype == np.float16 and f["ptype"].dtype == np.int8
+    assert int(f["step"]) == 1 and float(f["dx"]) == np.float32(cfg.dx)
+    assert np.array_equal(f["phi"], sim.phi_cell.numpy().astype(np.float16))
+    assert np.array_equal(f["px"], sim.px.numpy()[::3].astype(np.float16))
+    assert np.array_equal(f["ptype"], pt[::3].astype(np.int8))
+    io.save_frame(sim, str(tmp_path / "f2.npz"), particles=False)
+    assert set(io.load_frame(str(tmp_path / "f2.npz"))) == {"t", "step", "dx", "phi"}
