@@ -195,3 +195,44 @@ def test_solver_reuse_across_sizes_and_repeated_calls():
     r1 = g.solve(dev(b), x1, tol=1e-6)
     r2 = g.solve(dev(b), x2, tol=1e-6)
     assert r1 == r2 and np.array_equal(x1.numpy(), x2.numpy())
+
+
+@pytest.mark.parametrize("precision", ["fp16", "bf16"])
+@pytest.mark.parametrize("res", [(32, 32, 32), (24, 40, 36)])
+def test_mixed_precision_hierarchy_solves_to_fp64_accuracy(precision, res):
+    """16-bit hierarchy (FP32 outer CG, FP64 dots and coarsest): the solve
+    reaches 1e-6 in at most 1.5x the FP32 iterations (+4), and the solution
+    matches the FP64 oracle solved to 1e-12 within 10 * tol."""
+    bx, by, bz, b, _ = scenes.solve_problem(res, seed=9)
+    its = {}
+    for prec in ("fp32", precision):
+        g = MGPCG(res, DEV, pre=3, post=3, precision=prec)
+        g.build_hierarchy(dev(bx), dev(by), dev(bz))
+        x = DeviceArray.zeros(res, device=DEV)
+        it, rel = g.solve(dev(b), x, tol=1e-6, max_iter=200)
+        assert rel < 1e-6, (prec, it, rel)
+        its[prec] = (it, x.numpy())
+    assert its[precision][0] <= 1.5 * its["fp32"][0] + 4, its
+    x64, _, _ = O.fp64_reference_solve(bx, by, bz, b.astype(np.float64), tol=1e-12)
+    assert rel_err(its[precision][1], x64) < 1e-5
+
+
+@pytest.mark.parametrize("precision", ["fp16", "bf16"])
+def test_mixed_precision_step_matches_fp32_step(precision):
+    """One 32^3 dam-break step with the 16-bit hierarchy against the FP32 step:
+    both solve to 1e-6, so the projected fields and particles agree to solver
+    accuracy."""
+    from pfflip import Config, Simulator
+
+    out = {}
+    for prec in ("fp32", precision):
+        cfg = Config(res=(32,) * 3, dx=1 / 32, ppc=8, droplets=False, pcg_tol=1e-6, device=DEV, precision=prec)
+        sim = Simulator(cfg)
+        sim.set_particles(*scenes.dam_break(cfg))
+        rec = sim.step(0.5 * cfg.dx / np.sqrt(2 * 9.81 * 0.6))
+        assert rec["pcg_res"] < 1e-6
+        out[prec] = (sim.px.numpy(), sim.pressure.numpy(), rec["max_div"])
+    assert np.abs(out[precision][0] - out["fp32"][0]).max() < 1e-4 / 32
+    p32 = out["fp32"][1] - out["fp32"][1].mean()
+    pm = out[precision][1] - out[precision][1].mean()
+    assert rel_err(pm, p32) < 1e-5
