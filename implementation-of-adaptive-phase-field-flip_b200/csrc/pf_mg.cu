@@ -121,10 +121,12 @@ __global__ void k_level_coefs(int nx, int ny, int nz, const float* __restrict__ 
   const long long nc = (long long)nx * ny * nz;
   const long long nfx = (long long)(nx + 1) * ny * nz, nfy = (long long)nx * (ny + 1) * nz,
                   nfz = (long long)nx * ny * (nz + 1);
-  if (bz_pad) {
+  if (bz_pad) {  // fp32 hierarchy: fp32 rows; 16-bit hierarchy: the scaled 16-bit z-faces in the same buffer
     for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nfz; f += (long long)gridDim.x * blockDim.x) {
       const long long row = f / (nz + 1);
-      bz_pad[row * bz_pitch + (f - row * (nz + 1))] = bz[f];
+      const long long o = row * bz_pitch + (f - row * (nz + 1));
+      if (bz_lp) stT(reinterpret_cast<T*>(bz_pad) + o, bz[f] * lp_scale);
+      else bz_pad[o] = bz[f];
     }
   }
   const long long tot = nc + (bx_lp ? nfx + nfy + nfz : 0);
@@ -468,11 +470,15 @@ constexpr unsigned kTmaWaitLimit = 1u << 22;
 // One staged tile of the red-black sweep: prolongation folded into the staged
 // p (first post-sweep), colour 1 on the tile and its ring, colour 2 on the
 // tile, write-back of the tile to p_out (msum += the written values).
-template <int TI, int NT>
-__device__ __forceinline__ void tma_tile_sweep(float* sP, const float* sB, const float* sX, const float* sY,
-                                               const float* sZ, const SweepArgs<float, float>& a, int k0, int j0,
-                                               int i0, double& msum) {
+//   FS, FW, FX0: element type, row width and k offset (the row starts at
+//   k0 - FX0) of the staged faces; BS, BW, BX0 the same for b.  p is staged as
+//   float rows of TM_W starting at k0 - TM_X0.
+template <int TI, int NT, class T, class TB, class FS = float, int FW = TM_W, int FX0 = TM_X0, class BS = float,
+          int BW = TM_W, int BX0 = TM_X0>
+__device__ __forceinline__ void tma_tile_sweep(float* sP, const BS* sB, const FS* sX, const FS* sY, const FS* sZ,
+                                               const SweepArgs<T, TB>& a, int k0, int j0, int i0, double& msum) {
   using D = TmaDims<TI>;
+  const float bsc = a.b_scale ? *a.b_scale : 1.f;
   const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
   const int tid = threadIdx.x;
   const long long sI = (long long)n1 * n2;
@@ -482,7 +488,7 @@ __device__ __forceinline__ void tma_tile_sweep(float* sP, const float* sB, const
       const int c = e % TM_W, t = e / TM_W, r = t % D::PJ, q = t / D::PJ;
       const int i = i0 - 2 + q, j = j0 - 2 + r, k = k0 - TM_X0 + c;
       if (i >= 0 && i < n0 && j >= 0 && j < n1 && k >= 0 && k < n2)
-        sP[e] += a.pc[((long long)(i >> 1) * hn1 + (j >> 1)) * hn2 + (k >> 1)] * a.pc_scale;
+        sP[e] += ldT(a.pc + ((long long)(i >> 1) * hn1 + (j >> 1)) * hn2 + (k >> 1)) * a.pc_scale;
     }
     __syncthreads();
   }
@@ -490,14 +496,15 @@ __device__ __forceinline__ void tma_tile_sweep(float* sP, const float* sB, const
   // relax the cell at coefficient-frame coordinates (q, r, c), c = k - (k0 - 1)
   auto relax = [&](int q, int r, int c) {
     float* pp = sP + ((q + 1) * D::PJ + (r + 1)) * TM_W + (c + TM_X0 - 1);
-    const int ce = (q * D::CJ + r) * TM_W + (c + TM_X0 - 1);
-    const float bxl = sX[ce], bxu = sX[ce + D::CJ * TM_W];
-    const int ye = (q * (D::CJ + 1) + r) * TM_W + (c + TM_X0 - 1);
-    const float byl = sY[ye], byu = sY[ye + TM_W];
-    const float bzl = sZ[ce], bzu = sZ[ce + 1];
+    const int ce = (q * D::CJ + r) * FW + (c + FX0 - 1);
+    const float bxl = ldT(sX + ce), bxu = ldT(sX + ce + D::CJ * FW);
+    const int ye = (q * (D::CJ + 1) + r) * FW + (c + FX0 - 1);
+    const float byl = ldT(sY + ye), byu = ldT(sY + ye + FW);
+    const float bzl = ldT(sZ + ce), bzu = ldT(sZ + ce + 1);
+    const float bb = ldT(sB + (q * D::CJ + r) * BW + (c + BX0 - 1)) * bsc;
     bool ok;
     const float v = gs_update(*pp, pp[-D::PJ * TM_W], pp[D::PJ * TM_W], pp[-TM_W], pp[TM_W], pp[-1], pp[1], bxl, bxu,
-                              byl, byu, bzl, bzu, sB[ce], a.omega, a.flux, &ok);
+                              byl, byu, bzl, bzu, bb, a.omega, a.flux, &ok);
     if (ok) *pp = v;
   };
   const int c1 = a.first_color, c2 = c1 ^ 1;
@@ -545,15 +552,15 @@ __device__ __forceinline__ void tma_tile_sweep(float* sP, const float* sB, const
     const int i = i0 + q, j = j0 + r, k = k0 + c;
     if (i >= n0 || j >= n1 || k >= n2) continue;
     const float v = sP[((q + 2) * D::PJ + (r + 2)) * TM_W + (c + TM_X0)];
-    a.p_out[i * sI + (long long)j * n2 + k] = v;
-    if (a.partials) msum += (double)v;
+    stT(a.p_out + i * sI + (long long)j * n2 + k, v);
+    if (a.partials) msum += (double)roundT<T>(v);
   }
 }
 
 // mean of p_out over the grid: one partial per CTA, the last CTA sums them in
 // order and stores the shift in the solver state
-template <int NT>
-__device__ __forceinline__ void sweep_mean_finish(const SweepArgs<float, float>& a, double msum, double* sred) {
+template <int NT, class T, class TB>
+__device__ __forceinline__ void sweep_mean_finish(const SweepArgs<T, TB>& a, double msum, double* sred) {
   const int tid = threadIdx.x;
   if (a.partials) {
     const double bs = block_sum<NT>(msum, sred);
@@ -573,7 +580,7 @@ __device__ __forceinline__ void sweep_mean_finish(const SweepArgs<float, float>&
       v = block_sum<NT>(v, sred);
       if (tid == 0) {
         a.st->sum_last = v;
-        a.st->c_shift = (float)(-(v / (double)a.n_total));
+        a.st->c_shift = (float)(-(v / (double)a.n_total) * (a.mixed ? (double)a.st->zscale : 1.0));
         *a.counter = 0u;
       }
     }
@@ -640,7 +647,95 @@ __global__ void __launch_bounds__(NT) k_rb_tile_tma(const __grid_constant__ Tile
     return;
   }
   double msum = 0.0;
-  tma_tile_sweep<TI, NT>(sP, sB, sX, sY, sZ, a, k0, j0, i0, msum);
+  tma_tile_sweep<TI, NT, float, float>(sP, sB, sX, sY, sZ, a, k0, j0, i0, msum);
+  sweep_mean_finish<NT>(a, msum, sred);
+}
+
+// --------------------------------------------------------------- TMA-staged sweep (16-bit hierarchy)
+// The same sweep over FP16/BF16 levels.  16-bit rows are 48 elements (96 bytes)
+// from k0 - 8, so every x coordinate stays a multiple of 16 bytes; b comes in
+// as fp32 rows of 40 from k0 - 4 on the finest level (the FP32 residual) and
+// as 16-bit rows elsewhere.  p is staged raw and widened once into fp32 rows,
+// so both colours relax in fp32 exactly as k_rb_tile does; faces and b are
+// widened where they are read.  The z-faces come from the padded 16-bit copy
+// k_level_coefs writes into the level's bz_pad buffer.
+constexpr int TM16_W = 48, TM16_X0 = 8;
+
+template <int TI, bool B32> struct Tma16Dims {
+  static constexpr int PI = TI + 4, PJ = SW_TJ + 4, CI = TI + 2, CJ = SW_TJ + 2;
+  static constexpr int BW = B32 ? TM_W : TM16_W, BES = B32 ? 4 : 2;
+  static constexpr int P16N = PI * PJ * TM16_W, P32N = PI * PJ * TM_W, BN = CI * CJ * BW;
+  static constexpr int XN = (CI + 1) * CJ * TM16_W, YN = CI * (CJ + 1) * TM16_W, ZN = CI * CJ * TM16_W;
+  static constexpr int r128(int b) { return (b + 127) / 128 * 128; }
+  static constexpr int OFF_P32 = r128(P16N * 2), OFF_B = OFF_P32 + r128(P32N * 4), OFF_X = OFF_B + r128(BN * BES),
+                       OFF_Y = OFF_X + r128(XN * 2), OFF_Z = OFF_Y + r128(YN * 2), OFF_BAR = OFF_Z + r128(ZN * 2);
+  static constexpr size_t SMEM = OFF_BAR + 128 + 128;
+};
+
+template <int TI, int NT, class T, class TB>
+__global__ void __launch_bounds__(NT) k_rb_tile_tma16(const __grid_constant__ TileMaps maps, SweepArgs<T, TB> a) {
+  if (is_done(a.st)) return;
+  constexpr bool B32 = std::is_same<TB, float>::value;
+  using D = TmaDims<TI>;
+  using E = Tma16Dims<TI, B32>;
+  extern __shared__ __align__(128) unsigned char hsm_raw[];
+  unsigned char* hsm = hsm_raw + ((128u - (smem_u32(hsm_raw) & 127u)) & 127u);
+  T* sP16 = reinterpret_cast<T*>(hsm);
+  float* sP = reinterpret_cast<float*>(hsm + E::OFF_P32);
+  TB* sB = reinterpret_cast<TB*>(hsm + E::OFF_B);
+  T* sX = reinterpret_cast<T*>(hsm + E::OFF_X);
+  T* sY = reinterpret_cast<T*>(hsm + E::OFF_Y);
+  T* sZ = reinterpret_cast<T*>(hsm + E::OFF_Z);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(hsm + E::OFF_BAR);
+  __shared__ double sred[40];
+  __shared__ int s_fail;
+  const int k0 = blockIdx.x * SW_TK, j0 = blockIdx.y * SW_TJ, i0 = blockIdx.z * TI;
+  const int tid = threadIdx.x;
+  const bool load_p = !a.zero_in;
+  if (tid == 0) {
+    s_fail = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    const unsigned bytes =
+        (unsigned)((load_p ? E::P16N * 2 : 0) + E::BN * E::BES + (E::XN + E::YN + E::ZN) * 2);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    const int x16 = k0 - TM16_X0, xb = B32 ? k0 - TM_X0 : k0 - TM16_X0;
+    if (load_p) tma_load_3d(sP16, &maps.p, x16, j0 - 2, i0 - 2, bar);
+    tma_load_3d(sB, &maps.b, xb, j0 - 1, i0 - 1, bar);
+    tma_load_3d(sX, &maps.x, x16, j0 - 1, i0 - 1, bar);
+    tma_load_3d(sY, &maps.y, x16, j0 - 1, i0 - 1, bar);
+    tma_load_3d(sZ, &maps.z, x16, j0 - 1, i0 - 1, bar);
+  }
+  __syncthreads();  // barrier initialised before anyone waits on it
+  {
+    unsigned it = 0;
+    while (!mbar_try_wait(bar, 0)) {
+      if (++it > kTmaWaitLimit) {
+        s_fail = 1;
+        break;
+      }
+    }
+  }
+  __syncthreads();
+  if (s_fail) {
+    if (tid == 0 && a.st) {
+      a.st->status = ST_TMA_TIMEOUT;
+      a.st->done = 1;
+    }
+    unsigned it = 0;  // give the copies in flight a last bounded chance to land
+    while (!mbar_try_wait(bar, 0) && ++it < kTmaWaitLimit) {
+    }
+    return;
+  }
+  for (int e = tid; e < D::PN; e += NT) {  // p: 16-bit rows from k0 - 8 -> fp32 rows from k0 - 4
+    const int row = e / TM_W, c = e - row * TM_W;
+    sP[e] = load_p ? ldT(sP16 + row * TM16_W + c + (TM16_X0 - TM_X0)) : 0.f;
+  }
+  __syncthreads();
+  double msum = 0.0;
+  tma_tile_sweep<TI, NT, T, TB, T, TM16_W, TM16_X0, TB, E::BW, (B32 ? TM_X0 : TM16_X0)>(sP, sB, sX, sY, sZ, a, k0,
+                                                                                       j0, i0, msum);
   sweep_mean_finish<NT>(a, msum, sred);
 }
 
@@ -1579,18 +1674,26 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
+// 3D tensor of dtype (esize bytes per element): extents (d0 innermost, d1,
+// d2), row pitch and plane pitch in elements
+bool encode3d_t(CUtensorMap* m, CUtensorMapDataType dtype, uint32_t esize, const void* base, uint64_t d0, uint64_t d1,
+                uint64_t d2, uint64_t row_pitch, uint64_t plane_pitch, uint32_t b0, uint32_t b1, uint32_t b2) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn || !aligned16(base) || (row_pitch * esize) % 16 || (plane_pitch * esize) % 16 || (b0 * esize) % 16)
+    return false;
+  cuuint64_t dims[3] = {d0, d1, d2};
+  cuuint64_t strides[2] = {row_pitch * esize, plane_pitch * esize};
+  cuuint32_t box[3] = {b0, b1, b2};
+  cuuint32_t es[3] = {1, 1, 1};
+  return fn(m, dtype, 3, const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // 3D fp32 tensor: extents (d0 innermost, d1, d2), row pitch and plane pitch in floats
 bool encode3d(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint64_t d2, uint64_t row_pitch,
               uint64_t plane_pitch, uint32_t b0, uint32_t b1, uint32_t b2) {
-  EncodeTiledFn fn = encode_fn();
-  if (!fn || !aligned16(base) || (row_pitch * 4) % 16 || (plane_pitch * 4) % 16) return false;
-  cuuint64_t dims[3] = {d0, d1, d2};
-  cuuint64_t strides[2] = {row_pitch * 4, plane_pitch * 4};
-  cuuint32_t box[3] = {b0, b1, b2};
-  cuuint32_t es[3] = {1, 1, 1};
-  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base), dims, strides, box, es,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  return encode3d_t(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, d0, d1, d2, row_pitch, plane_pitch, b0, b1, b2);
 }
 
 // TMA staging of a level: fp32 storage, rows a multiple of 4 floats, padded z-faces
@@ -1609,6 +1712,32 @@ bool tma_maps(pf_mg_plan* P, int lv, const T* p_in, const TB* b, const float* b_
            encode3d(&m->y, V.by, n2, n1 + 1, n0, n2, (n1 + 1) * n2, TM_W, SW_TJ + 3, TI + 2) &&
            encode3d(&m->z, L.bz_pad, n2 + 1, n1, n0, (uint64_t)L.bz_pitch, n1 * (uint64_t)L.bz_pitch, TM_W,
                     SW_TJ + 2, TI + 2);
+  }
+}
+
+// TMA staging of a 16-bit level: rows a multiple of 8 elements (16 bytes), the
+// padded 16-bit z-faces in bz_pad; b is the fp32 residual (finest level, with
+// its scale) or 16-bit
+template <int TI, class T, class TB>
+bool tma_maps16(pf_mg_plan* P, int lv, const T* p_in, const TB* b, const LV<T>& V, TileMaps* m) {
+  if constexpr (std::is_same<T, float>::value) {
+    return false;
+  } else {
+    const pf_mg_level& L = P->d.lev[lv];
+    if (!L.bz_pad || L.nz % 8 != 0 || L.bz_pitch % 8 != 0) return false;
+    const CUtensorMapDataType dt =
+        std::is_same<T, __half>::value ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    const uint64_t n0 = L.nx, n1 = L.ny, n2 = L.nz;
+    const T* pm = p_in ? p_in : V.p0;
+    bool ok = encode3d_t(&m->p, dt, 2, pm, n2, n1, n0, n2, n1 * n2, TM16_W, SW_TJ + 4, TI + 4);
+    if constexpr (std::is_same<TB, float>::value)
+      ok = ok && encode3d(&m->b, b, n2, n1, n0, n2, n1 * n2, TM_W, SW_TJ + 2, TI + 2);
+    else
+      ok = ok && encode3d_t(&m->b, dt, 2, b, n2, n1, n0, n2, n1 * n2, TM16_W, SW_TJ + 2, TI + 2);
+    return ok && encode3d_t(&m->x, dt, 2, V.bx, n2, n1, n0 + 1, n2, n1 * n2, TM16_W, SW_TJ + 2, TI + 3) &&
+           encode3d_t(&m->y, dt, 2, V.by, n2, n1 + 1, n0, n2, (n1 + 1) * n2, TM16_W, SW_TJ + 3, TI + 2) &&
+           encode3d_t(&m->z, dt, 2, L.bz_pad, n2 + 1, n1, n0, (uint64_t)L.bz_pitch, n1 * (uint64_t)L.bz_pitch,
+                      TM16_W, SW_TJ + 2, TI + 2);
   }
 }
 
@@ -1645,6 +1774,15 @@ int launch_sweep(pf_mg_plan* P, int lv, const T* p_in, bool zero_in, T* p_out, c
     }
     if (P->use_tma && tma_maps<TI, T, TB>(P, lv, p_in, b, b_scale, V, &maps)) {
       k_rb_tile_tma<TI, SW_NT><<<grid, SW_NT, TmaDims<TI>::SMEM, s>>>(maps, a);
+      PF_LAUNCHED();
+      return PF_OK;
+    }
+  }
+  if constexpr (!std::is_same<T, float>::value) {
+    TileMaps maps;
+    if (P->use_tma && tma_maps16<TI, T, TB>(P, lv, p_in, b, V, &maps)) {
+      k_rb_tile_tma16<TI, SW_NT, T, TB>
+          <<<grid, SW_NT, Tma16Dims<TI, std::is_same<TB, float>::value>::SMEM, s>>>(maps, a);
       PF_LAUNCHED();
       return PF_OK;
     }
@@ -1972,6 +2110,12 @@ template <class T> cudaError_t set_smem_attrs() {
   chk(cudaFuncSetAttribute(k_rb_tile_tma<4, SW_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)TmaDims<4>::SMEM));
   chk(cudaFuncSetAttribute(k_rb_tile_tma<8, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TmaDims<8>::SMEM));
+  if constexpr (!std::is_same<T, float>::value) {
+    chk(cudaFuncSetAttribute(k_rb_tile_tma16<4, SW_NT, T, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)Tma16Dims<4, true>::SMEM));
+    chk(cudaFuncSetAttribute(k_rb_tile_tma16<4, SW_NT, T, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)Tma16Dims<4, false>::SMEM));
+  }
   return e;
 }
 
