@@ -833,7 +833,8 @@ template <class T, class TB> struct BottomArgs {
   int flux;
   MGState* st;
   int want_mean, mixed;
-  int bulk;  // stage faces and b with cp.async.bulk (fp32 storage, 16-byte sizes)
+  int bulk;  // stage faces and b with cp.async.bulk: 1 = fp32 storage straight into the level arrays,
+             // 2 = 16-bit storage into a staging area behind Pc, widened there (16-byte sizes)
 };
 
 __host__ __device__ inline size_t bottom_level_floats(int n0, int n1, int n2) {
@@ -913,6 +914,10 @@ __device__ __forceinline__ void bt_coarsest_regs(const BottomLevel& L, R* P, con
   const int h = l % hk, row = l / hk, j = row % n1, i = row / n1;
   const int sI = n1 * n2;
   float cx0[2], cx1[2], cy0[2], cy1[2], cz0[2], cz1[2], cb[2], cd[2];  // as stored; widened at use
+  // FP64 (16-bit hierarchy): omega/d once per cell instead of a division per
+  // relaxation; FP32 keeps bt_relax's omega*res/d
+  constexpr bool kRecip = std::is_same<R, double>::value;
+  R cw[2];
   R p[2];
 #pragma unroll
   for (int s = 0; s < 2; ++s) {
@@ -926,6 +931,7 @@ __device__ __forceinline__ void bt_coarsest_regs(const BottomLevel& L, R* P, con
     cz1[s] = Z[fzi + 1];
     cd[s] = X[e] + X[e + sI] + Y[fyi] + Y[fyi + n2] + Z[fzi] + Z[fzi + 1];
     cb[s] = B[e];
+    cw[s] = kRecip ? omega / (R)cd[s] : R(0);
     p[s] = act ? P[2 * l + s] : R(0);
   }
   const int di = n1 * hk;
@@ -967,7 +973,8 @@ __device__ __forceinline__ void bt_coarsest_regs(const BottomLevel& L, R* P, con
         sum += bzu * q5;
         res = bb - (d * pv - sum);
       }
-      const R nv = (act && d > R(0)) ? pv + omega * res / d : pv;
+      R nv = pv;
+      if (act && d > R(0)) nv = kRecip ? pv + res * (sc ? cw[1] : cw[0]) : pv + omega * res / d;
       if (sc) p[1] = nv;
       else p[0] = nv;
     }
@@ -1055,43 +1062,65 @@ __global__ void __launch_bounds__(BT_NT) k_bottom(BottomArgs<T, TB> a) {
     return r;
   };
   AccT* Pc;
+  unsigned char* stg;  // 16-bit staging (bulk == 2)
   {
     float* end = base(nl);
     Pc = reinterpret_cast<AccT*>((reinterpret_cast<uintptr_t>(end) + 15) & ~uintptr_t(15));
+    const BottomLevel& Lc = a.L[nl - 1];
+    stg = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(Pc + Lc.n0 * Lc.n1 * Lc.n2) + 15) & ~uintptr_t(15));
   }
   // ---- load faces of every level and b of the top level; zero p
   if (a.bulk) {
     // one thread issues a bulk copy per array (the host checked that every
-    // array is fp32, 16-byte aligned and a multiple of 16 bytes long); all
-    // complete on one mbarrier, waited on with a bound
+    // array is 16-byte aligned and a multiple of 16 bytes long); all complete
+    // on one mbarrier, waited on with a bound.  fp32 arrays land in place;
+    // 16-bit arrays land back to back in the staging area and are widened
+    // after the wait
     __shared__ __align__(8) uint64_t bt_bar;
     __shared__ int bt_fail;
+    const bool wide = a.bulk == 1;
+    constexpr unsigned kES = sizeof(T), kBS = sizeof(TB);
     if (tid == 0) {
       bt_fail = 0;
-      unsigned bytes = 4u * (unsigned)(a.L[0].n0 * a.L[0].n1 * a.L[0].n2);
+      unsigned bytes = (wide ? 4u : kBS) * (unsigned)(a.L[0].n0 * a.L[0].n1 * a.L[0].n2);
       for (int l = 0; l < nl; ++l) {
         const BottomLevel& L = a.L[l];
-        bytes += 4u * (unsigned)((L.n0 + 1) * L.n1 * L.n2 + L.n0 * (L.n1 + 1) * L.n2 + L.n0 * L.n1 * (L.n2 + 1));
+        bytes += (wide ? 4u : kES) *
+                 (unsigned)((L.n0 + 1) * L.n1 * L.n2 + L.n0 * (L.n1 + 1) * L.n2 + L.n0 * L.n1 * (L.n2 + 1));
       }
       const unsigned bar = smem_u32(&bt_bar);
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-      auto bulk = [&](float* dst, const void* src, int count) {
+      auto bulk = [&](void* dst, const void* src, unsigned nbytes) {
         asm volatile(
             "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                 smem_u32(dst)),
-            "l"(reinterpret_cast<uint64_t>(src)), "r"(4 * count), "r"(bar)
+            "l"(reinterpret_cast<uint64_t>(src)), "r"(nbytes), "r"(bar)
             : "memory");
       };
+      unsigned char* sp = stg;
       for (int l = 0; l < nl; ++l) {
         const BottomLevel& L = a.L[l];
         const LvPtr q = ptrs(l);
-        bulk(q.X, L.bx, (L.n0 + 1) * L.n1 * L.n2);
-        bulk(q.Y, L.by, L.n0 * (L.n1 + 1) * L.n2);
-        bulk(q.Z, L.bz, L.n0 * L.n1 * (L.n2 + 1));
+        const unsigned nx = (L.n0 + 1) * L.n1 * L.n2, ny = L.n0 * (L.n1 + 1) * L.n2, nz = L.n0 * L.n1 * (L.n2 + 1);
+        if (wide) {
+          bulk(q.X, L.bx, 4u * nx);
+          bulk(q.Y, L.by, 4u * ny);
+          bulk(q.Z, L.bz, 4u * nz);
+        } else {
+          bulk(sp, L.bx, kES * nx);
+          sp += kES * nx;
+          bulk(sp, L.by, kES * ny);
+          sp += kES * ny;
+          bulk(sp, L.bz, kES * nz);
+          sp += kES * nz;
+        }
       }
-      bulk(ptrs(0).B, a.b, a.L[0].n0 * a.L[0].n1 * a.L[0].n2);
+      const unsigned n0c = a.L[0].n0 * a.L[0].n1 * a.L[0].n2;
+      if (wide) bulk(ptrs(0).B, a.b, 4u * n0c);
+      else bulk(sp, a.b, kBS * n0c);
     }
     for (int l = 0; l < nl; ++l) {
       const LvPtr q = ptrs(l);
@@ -1118,6 +1147,22 @@ __global__ void __launch_bounds__(BT_NT) k_bottom(BottomArgs<T, TB> a) {
       while (!mbar_try_wait(&bt_bar, 0) && ++it < kTmaWaitLimit) {
       }
       return;
+    }
+    if (!wide) {  // widen the staged 16-bit faces and b
+      const T* sp = reinterpret_cast<const T*>(stg);
+      for (int l = 0; l < nl; ++l) {
+        const BottomLevel& L = a.L[l];
+        const LvPtr q = ptrs(l);
+        const int nf = (L.n0 + 1) * L.n1 * L.n2 + L.n0 * (L.n1 + 1) * L.n2 + L.n0 * L.n1 * (L.n2 + 1);
+        for (int e = tid; e < nf; e += BT_NT) q.X[e] = ldT(sp + e);  // X, Y, Z are contiguous
+        sp += nf;
+      }
+      const float bsc = a.b_scale ? *a.b_scale : 1.f;
+      const TB* sb = reinterpret_cast<const TB*>(sp);
+      const LvPtr q = ptrs(0);
+      const int n0c = a.L[0].n0 * a.L[0].n1 * a.L[0].n2;
+      for (int e = tid; e < n0c; e += BT_NT) q.B[e] = ldT(sb + e) * bsc;
+      __syncthreads();
     }
   } else {
     for (int l = 0; l < nl; ++l) {
@@ -1621,6 +1666,7 @@ struct pf_mg_plan {
   bool use_tma;        // stage fp32 smoother tiles with TMA where the level allows it
   int sms;             // multiprocessors of the plan's device (persistent sweep grid)
   size_t bottom_smem;  // dynamic shared memory of the bottom kernel
+  bool bottom_stage;   // bottom_smem includes the 16-bit staging area
   cudaStream_t cap_stream;
   cudaGraphExec_t exec[2];
   size_t exec_nodes[2];
@@ -1780,6 +1826,13 @@ int launch_sweep(pf_mg_plan* P, int lv, const T* p_in, bool zero_in, T* p_out, c
   }
   if constexpr (!std::is_same<T, float>::value) {
     TileMaps maps;
+    constexpr bool B32 = std::is_same<TB, float>::value;
+    if (P->use_tma && L.nx >= 128 && tma_maps16<8, T, TB>(P, lv, p_in, b, V, &maps)) {
+      const dim3 g8(grid.x, grid.y, (L.nx + 7) / 8);
+      k_rb_tile_tma16<8, 512, T, TB><<<g8, 512, Tma16Dims<8, B32>::SMEM, s>>>(maps, a);
+      PF_LAUNCHED();
+      return PF_OK;
+    }
     if (P->use_tma && tma_maps16<TI, T, TB>(P, lv, p_in, b, V, &maps)) {
       k_rb_tile_tma16<TI, SW_NT, T, TB>
           <<<grid, SW_NT, Tma16Dims<TI, std::is_same<TB, float>::value>::SMEM, s>>>(maps, a);
@@ -1835,6 +1888,16 @@ int launch_bottom(pf_mg_plan* P, const TB* b, const float* b_scale, bool want_me
       for (int c = 0; c < 3; ++c) ok = ok && aligned16(ptr[c]) && (nf[c] * 4) % 16 == 0;
     }
     a.bulk = ok ? 1 : 0;
+  } else {
+    bool ok = aligned16(b) && ((size_t)ncells(P->d.lev[lb]) * sizeof(TB)) % 16 == 0 && P->bottom_stage;
+    for (int l = 0; l < a.nl && ok; ++l) {
+      const BottomLevel& L = a.L[l];
+      const long long nf[3] = {(long long)(L.n0 + 1) * L.n1 * L.n2, (long long)L.n0 * (L.n1 + 1) * L.n2,
+                               (long long)L.n0 * L.n1 * (L.n2 + 1)};
+      const void* ptr[3] = {L.bx, L.by, L.bz};
+      for (int c = 0; c < 3; ++c) ok = ok && aligned16(ptr[c]) && (nf[c] * (long long)sizeof(T)) % 16 == 0;
+    }
+    a.bulk = ok ? 2 : 0;
   }
   if (mixed(P)) k_bottom<T, TB, double><<<1, BT_NT, P->bottom_smem, s>>>(a);
   else k_bottom<T, TB, float><<<1, BT_NT, P->bottom_smem, s>>>(a);
@@ -2115,6 +2178,10 @@ template <class T> cudaError_t set_smem_attrs() {
                              (int)Tma16Dims<4, true>::SMEM));
     chk(cudaFuncSetAttribute(k_rb_tile_tma16<4, SW_NT, T, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)Tma16Dims<4, false>::SMEM));
+    chk(cudaFuncSetAttribute(k_rb_tile_tma16<8, 512, T, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)Tma16Dims<8, true>::SMEM));
+    chk(cudaFuncSetAttribute(k_rb_tile_tma16<8, 512, T, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)Tma16Dims<8, false>::SMEM));
   }
   return e;
 }
@@ -2182,16 +2249,22 @@ int pf_mg_plan_create(const pf_mg_desc* desc, pf_mg_plan** out) {
   // together fit the shared memory of one CTA
   P->lb = desc->nlev;
   P->bottom_smem = 0;
+  P->bottom_stage = desc->precision != PF_PREC_FP32;
   {
-    size_t floats = 0;
+    // 16-bit hierarchy: a staging area for the raw 16-bit faces (and b, at
+    // most 4 bytes a cell) behind the coarsest solution
+    size_t floats = 0, faces = 0;
     const pf_mg_level& Lc = desc->lev[desc->nlev - 1];
     for (int lv = desc->nlev - 1; lv >= 0; --lv) {
       const pf_mg_level& L = desc->lev[lv];
       const long long n = (long long)L.nx * L.ny * L.nz;
       const size_t f2 = floats + bottom_level_floats(L.nx, L.ny, L.nz);
-      const size_t bytes = f2 * sizeof(float) + 16 + (size_t)Lc.nx * Lc.ny * Lc.nz * sizeof(double);
+      const size_t fc2 = faces + bottom_level_floats(L.nx, L.ny, L.nz) - 2 * (size_t)n;
+      const size_t stage = P->bottom_stage ? 16 + 2 * fc2 + 4 * (size_t)n : 0;
+      const size_t bytes = f2 * sizeof(float) + 16 + (size_t)Lc.nx * Lc.ny * Lc.nz * sizeof(double) + stage;
       if (n > kBottomMaxCells || bytes > 200 * 1024) break;
       floats = f2;
+      faces = fc2;
       P->lb = lv;
       P->bottom_smem = bytes;
     }
