@@ -12,6 +12,7 @@
 // for power-of-two dx, within an ulp otherwise.
 // Particles are in cell order, so neighbouring threads gather neighbouring
 // taps from L1/L2.
+#include "pf_f32x2.cuh"
 #include "pf_faces.cuh"
 
 namespace pf {
@@ -255,45 +256,49 @@ __device__ __forceinline__ void rows_of(const Frame& fr, int c, int ny, int nz, 
   r.clampk = fr.lo[2][vk] == fr.hi[2][vk];
 }
 
+// The samplers below run on packed f32x2 pairs: each row load gives the
+// (lower, upper) k taps as one pair, weighted by (w_ij w_k0, w_ij w_k1), and
+// the two halves are summed at the end.  Tap values and weights are the
+// unpaired kernel's; only the order of the final sum differs.
+
 // G2P sample of component c: delta = I(u - u*) tap by tap, pic = I(u)
 __device__ __forceinline__ void sample_g2p_packed(const float4* __restrict__ uu, const Rows& r, float& delta,
                                                   float& pic) {
-  float ad = 0.f, ap = 0.f;
+  const f2 wk = f2_make(r.wk0, r.wk1), neg1 = f2_bcast(-1.f);
+  f2 ad = f2_bcast(0.f), ap = ad;
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const float4 v = __ldg(uu + r.row[q]);
     const float u1 = r.clampk ? v.x : v.y, s1 = r.clampk ? v.z : v.w;
-    ad += r.wij[q] * r.wk0 * (v.x - v.z);
-    ad += r.wij[q] * r.wk1 * (u1 - s1);
-    ap += r.wij[q] * r.wk0 * v.x;
-    ap += r.wij[q] * r.wk1 * u1;
+    const f2 w = f2_mul(f2_bcast(r.wij[q]), wk);
+    const f2 u2 = f2_make(v.x, u1);
+    ad = f2_fma(w, f2_fma(f2_make(v.z, s1), neg1, u2), ad);
+    ap = f2_fma(w, u2, ap);
   }
-  delta = ad;
-  pic = ap;
+  delta = f2_x(ad) + f2_y(ad);
+  pic = f2_x(ap) + f2_y(ap);
 }
 
 __device__ __forceinline__ float sample_pair2(const float2* __restrict__ f, const Rows& r) {
-  float acc = 0.f;
+  const f2 wk = f2_make(r.wk0, r.wk1);
+  f2 acc = f2_bcast(0.f);
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const float2 v = __ldg(f + r.row[q]);
-    const float h = r.clampk ? v.x : v.y;
-    acc += r.wij[q] * r.wk0 * v.x;
-    acc += r.wij[q] * r.wk1 * h;
+    acc = f2_fma(f2_mul(f2_bcast(r.wij[q]), wk), f2_make(v.x, r.clampk ? v.x : v.y), acc);
   }
-  return acc;
+  return f2_x(acc) + f2_y(acc);
 }
 
 __device__ __forceinline__ float sample_pair4(const float4* __restrict__ f, const Rows& r) {
-  float acc = 0.f;
+  const f2 wk = f2_make(r.wk0, r.wk1);
+  f2 acc = f2_bcast(0.f);
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const float4 v = __ldg(f + r.row[q]);
-    const float h = r.clampk ? v.x : v.y;
-    acc += r.wij[q] * r.wk0 * v.x;
-    acc += r.wij[q] * r.wk1 * h;
+    acc = f2_fma(f2_mul(f2_bcast(r.wij[q]), wk), f2_make(v.x, r.clampk ? v.x : v.y), acc);
   }
-  return acc;
+  return f2_x(acc) + f2_y(acc);
 }
 
 // RK3 sample: liquid particles read the extrapolated field, air the raw one

@@ -27,6 +27,7 @@
 #include <type_traits>
 #include <vector>
 
+#include <cooperative_groups.h>
 #include <cuda.h>
 
 #include "pf_common.cuh"
@@ -1017,20 +1018,169 @@ __device__ __forceinline__ void bt_half_sweep(const BottomLevel& L, R* P, const 
 }
 
 // dst[e] = src[e] (converted) for e < n, loads issued 8 at a time
-template <class T>
+template <class T, int NT = BT_NT>
 __device__ __forceinline__ void bt_load(float* dst, const T* src, int n, float scale, int tid) {
-  for (int base = tid; base < n; base += 8 * BT_NT) {
+  for (int base = tid; base < n; base += 8 * NT) {
     float v[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
-      const int e = base + u * BT_NT;
+      const int e = base + u * NT;
       v[u] = (e < n) ? ldT(src + e) * scale : 0.f;
     }
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
-      const int e = base + u * BT_NT;
+      const int e = base + u * NT;
       if (e < n) dst[e] = v[u];
     }
+  }
+}
+
+struct BtPtrs {
+  float *P, *B, *X, *Y, *Z;
+};
+
+// arrays of level l of a run of levels laid out back to back from base
+// (per level P, B, X, Y, Z in that order)
+__device__ __forceinline__ BtPtrs bt_ptrs(const BottomLevel* Ls, float* base, int l) {
+  size_t off = 0;
+  for (int q = 0; q < l; ++q) off += bottom_level_floats(Ls[q].n0, Ls[q].n1, Ls[q].n2);
+  const int n0 = Ls[l].n0, n1 = Ls[l].n1, n2 = Ls[l].n2, n = n0 * n1 * n2;
+  BtPtrs r;
+  r.P = base + off;
+  r.B = r.P + n;
+  r.X = r.B + n;
+  r.Y = r.X + (n0 + 1) * n1 * n2;
+  r.Z = r.Y + n0 * (n1 + 1) * n2;
+  return r;
+}
+
+// The V-cycle over levels l0 .. nl-1 held in one CTA's shared memory from
+// base (NT threads, CTA barriers only): level l0's B is set and every P is zero
+// on entry; level l0's P holds the result on return.  Pre-smoothing, residual
+// and restriction on the way down, `coarsest` sweeps from zero in AccT with the
+// mean removed, prolongation and post-smoothing with the colours reversed on
+// the way up (pfflip/poisson.py:312-345).
+template <class T, class AccT, int NT = BT_NT>
+__device__ void bt_local_vcycle(const BottomLevel* Ls, float* base, int l0, int nl, AccT* Pc, float om, int pre,
+                                int post, int coarsest, float rscale, float pscale, int flux, double* sred,
+                                double* s_mean) {
+  const int tid = threadIdx.x;
+  // ---- down: pre-smoothing, residual, restriction
+  for (int l = l0; l < nl - 1; ++l) {
+    const BottomLevel& L = Ls[l];
+    const BtPtrs q = bt_ptrs(Ls, base, l);
+    for (int sw = 0; sw < pre; ++sw)
+      for (int cc = 0; cc < 2; ++cc) {
+        bt_half_sweep<float>(L, q.P, q.B, q.X, q.Y, q.Z, cc, om, flux, tid, NT);
+        __syncthreads();
+      }
+    const int n0 = L.n0, n1 = L.n1, n2 = L.n2;
+    const int C1 = n1 >> 1, C2 = n2 >> 1, nc = (n0 >> 1) * C1 * C2;
+    float* Bc = bt_ptrs(Ls, base, l + 1).B;
+    const int sI = n1 * n2;
+    const bool p2 = L.s1 >= 1 && L.s2 >= 1;
+    for (int ec = tid; ec < nc; ec += NT) {
+      int I, J, K;
+      if (p2) {
+        K = ec & (C2 - 1);
+        const int t = ec >> (L.s2 - 1);
+        J = t & (C1 - 1);
+        I = t >> (L.s1 - 1);
+      } else {
+        K = ec % C2;
+        const int t = ec / C2;
+        J = t % C1;
+        I = t / C1;
+      }
+      float acc = 0.f;
+#pragma unroll
+      for (int aa = 0; aa < 2; ++aa)
+#pragma unroll
+        for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+          for (int cc = 0; cc < 2; ++cc) {
+            const int i = 2 * I + aa, j = 2 * J + bb, k = 2 * K + cc;
+            const int e = (i * n1 + j) * n2 + k;
+            const int fyi = (i * (n1 + 1) + j) * n2 + k, fzi = (i * n1 + j) * (n2 + 1) + k;
+            const float bxl = q.X[e], bxu = q.X[e + sI], byl = q.Y[fyi], byu = q.Y[fyi + n2], bzl = q.Z[fzi],
+                        bzu = q.Z[fzi + 1];
+            const float pv = q.P[e];
+            const float q0 = q.P[i > 0 ? e - sI : e], q1 = q.P[i < n0 - 1 ? e + sI : e];
+            const float q2 = q.P[j > 0 ? e - n2 : e], q3 = q.P[j < n1 - 1 ? e + n2 : e];
+            const float q4 = q.P[k > 0 ? e - 1 : e], q5 = q.P[k < n2 - 1 ? e + 1 : e];
+            float Ap;
+            if (flux) {
+              float sm = bxl * (pv - q0);
+              sm += bxu * (pv - q1);
+              sm += byl * (pv - q2);
+              sm += byu * (pv - q3);
+              sm += bzl * (pv - q4);
+              sm += bzu * (pv - q5);
+              Ap = sm;
+            } else {
+              const float d = bxl + bxu + byl + byu + bzl + bzu;
+              float sm = bxl * q0;
+              sm += bxu * q1;
+              sm += byl * q2;
+              sm += byu * q3;
+              sm += bzl * q4;
+              sm += bzu * q5;
+              Ap = d * pv - sm;
+            }
+            acc += q.B[e] - Ap;
+          }
+      Bc[ec] = roundT<T>(acc * rscale);
+    }
+    __syncthreads();
+  }
+  // ---- coarsest: sweeps from zero in AccT, then mean removal
+  {
+    const BottomLevel& L = Ls[nl - 1];
+    const BtPtrs q = bt_ptrs(Ls, base, nl - 1);
+    const int n = L.n0 * L.n1 * L.n2;
+    for (int e = tid; e < n; e += NT) Pc[e] = AccT(0);
+    __syncthreads();
+    const bool one_warp = n <= 256;
+    const AccT omc = (AccT)om;
+    if (n <= 64 && (L.n2 & 1) == 0) {
+      if (tid < 32) bt_coarsest_regs<AccT>(L, Pc, q.B, q.X, q.Y, q.Z, omc, coarsest, flux, tid);
+    } else if (!one_warp || tid < 32) {
+      const int nt = one_warp ? 32 : NT;
+      for (int sw = 0; sw < coarsest; ++sw) {
+        for (int color = 0; color < 2; ++color) {
+          bt_half_sweep<AccT>(L, Pc, q.B, q.X, q.Y, q.Z, color, omc, flux, tid, nt);
+          if (one_warp) __syncwarp();
+          else __syncthreads();
+        }
+      }
+    }
+    __syncthreads();
+    double ls = 0.0;
+    for (int e = tid; e < n; e += NT) ls += (double)Pc[e];
+    const double tot = block_sum<NT>(ls, sred);
+    if (tid == 0) *s_mean = tot / (double)n;
+    __syncthreads();
+    const AccT shift = (AccT)(-*s_mean);
+    for (int e = tid; e < n; e += NT) q.P[e] = roundT<T>((float)(Pc[e] + shift));
+    __syncthreads();
+  }
+  // ---- up: prolongation, post-smoothing with the colours reversed
+  for (int l = nl - 2; l >= l0; --l) {
+    const BottomLevel& L = Ls[l];
+    const BtPtrs q = bt_ptrs(Ls, base, l);
+    const float* Pcoarse = bt_ptrs(Ls, base, l + 1).P;
+    const int n = L.n0 * L.n1 * L.n2, h1 = L.n1 >> 1, h2 = L.n2 >> 1;
+    for (int e = tid; e < n; e += NT) {
+      int i, j, k;
+      bt_ijk(L, e, i, j, k);
+      q.P[e] += Pcoarse[((i >> 1) * h1 + (j >> 1)) * h2 + (k >> 1)] * pscale;
+    }
+    __syncthreads();
+    for (int sw = 0; sw < post; ++sw)
+      for (int cc = 0; cc < 2; ++cc) {
+        bt_half_sweep<float>(L, q.P, q.B, q.X, q.Y, q.Z, 1 ^ cc, om, flux, tid, NT);
+        __syncthreads();
+      }
   }
 }
 
@@ -1180,22 +1330,324 @@ __global__ void __launch_bounds__(BT_NT) k_bottom(BottomArgs<T, TB> a) {
     }
     __syncthreads();
   }
+  bt_local_vcycle<T, AccT>(a.L, reinterpret_cast<float*>(btsm), 0, nl, Pc, a.omega, a.pre, a.post, a.coarsest,
+                           a.rscale, a.pscale, a.flux, sred, &s_mean);
+  // ---- output (and the mean when the top level is level 0)
+  const float* P0 = ptrs(0).P;
+  const int n = a.L[0].n0 * a.L[0].n1 * a.L[0].n2;
+  double ls = 0.0;
+  for (int e = tid; e < n; e += BT_NT) {
+    stT(a.p_out + e, P0[e]);
+    ls += (double)roundT<T>(P0[e]);
+  }
+  if (a.want_mean) {
+    const double tot = block_sum<BT_NT>(ls, sred);
+    if (tid == 0) {
+      a.st->sum_last = tot;
+      a.st->c_shift = (float)(-(tot / (double)n) * (a.mixed ? (double)a.st->zscale : 1.0));
+    }
+  }
+}
+
+// --------------------------------------------------------------- bottom V-cycle on a CTA cluster
+// The coarse end of the V-cycle from a level of up to ~32^3 cells down, in one
+// launch of one cluster of BC_CTAS CTAs (distributed shared memory, no TMA).
+// The finer "distributed" levels are split into slabs of s = n0/BC_CTAS
+// planes along i, one slab per CTA, held in that CTA's shared memory with two
+// halo planes (the neighbours' boundary planes) in two slots.  After every
+// change of a slab (a half-sweep, a prolongation) each CTA writes its first
+// and last plane into the other slot of its neighbours' halos (distributed
+// shared memory stores), and one cluster barrier makes them visible: the next
+// half-sweep reads only local shared memory, and since a half-sweep reads the
+// slot the previous step wrote while the writes of its own step go to the
+// other slot, one barrier per half-sweep is enough.  Restriction and prolongation between distributed
+// levels stay inside a slab (s even); the coarsest distributed level
+// restricts into CTA 0, which runs the remaining levels alone with
+// bt_local_vcycle while the other CTAs wait at the next cluster barrier.
+// Arithmetic per cell is bt_relax's and the restriction's of k_bottom, with
+// the same colour orders.
+constexpr int BC_CTAS = 8;
+constexpr int BC_MAX_DIST = 4;
+constexpr int BC_NT = 512;  // threads per CTA (128 registers a thread)
+constexpr int kDenseMaxCells = 1024;  // largest level applied as a dense operator
+static_assert(kDenseMaxCells / BC_CTAS <= BC_NT, "dense rows of a CTA must fit its partial-sum buffer");
+
+template <class T, class TB> struct ClusterArgs {
+  int nd;                           // distributed levels, [0] = top
+  BottomLevel D[BC_MAX_DIST];
+  int nl;                           // levels on CTA 0, [0] = the one below D[nd-1]
+  BottomLevel L[PF_MG_MAX_LEVELS];
+  const TB* b;                      // right-hand side of D[0]
+  const float* b_scale;
+  T* p_out;                         // solution of D[0]
+  float omega;
+  int pre, post, coarsest;
+  float rscale, pscale;
+  int flux;
+  MGState* st;
+  int want_mean, mixed;
+  const float* M;                   // dense operator of the levels below (null: CTA 0 runs them)
+  int nb;                           // its size: cells of the level below D[nd-1]
+};
+
+// floats of one CTA's slab of a distributed level: P, B (s planes), X (s+1
+// face planes), Y, Z (s planes), H (2 slots x (lower, upper) halo planes)
+__host__ __device__ inline size_t bc_level_floats(int n0, int n1, int n2) {
+  const size_t s = (size_t)(n0 / BC_CTAS);
+  return 2 * s * n1 * n2 + (s + 1) * n1 * n2 + s * (n1 + 1) * n2 + s * n1 * (n2 + 1) + 4 * (size_t)n1 * n2;
+}
+
+// one CTA's slab of a distributed level: planes i0 .. i0+s-1; Plo / Phi point
+// at the current halo slot's copies of the last plane of the CTA below and the
+// first plane of the CTA above (unused at the domain walls)
+struct DLv {
+  float *P, *B, *X, *Y, *Z, *H;
+  const float* Plo;
+  const float* Phi;
+  int n0, n1, n2, s, i0;
+  int s1, s2;  // log2(n1), log2(n2) when both are powers of two, else -1
+  __device__ __forceinline__ void use_slot(int slot) {
+    Plo = H + (2 * slot) * n1 * n2;
+    Phi = Plo + n1 * n2;
+  }
+};
+
+__device__ __forceinline__ DLv bc_level(const BottomLevel* D, float* base, int l, int rank,
+                                        cooperative_groups::cluster_group& cl) {
+  size_t off = 0;
+  for (int q = 0; q < l; ++q) off += bc_level_floats(D[q].n0, D[q].n1, D[q].n2);
+  DLv v;
+  v.n0 = D[l].n0;
+  v.n1 = D[l].n1;
+  v.n2 = D[l].n2;
+  v.s = v.n0 / BC_CTAS;
+  v.i0 = rank * v.s;
+  v.s1 = D[l].s1;
+  v.s2 = D[l].s2;
+  const int pl = v.n1 * v.n2;
+  v.P = base + off;
+  v.B = v.P + v.s * pl;
+  v.X = v.B + v.s * pl;
+  v.Y = v.X + (v.s + 1) * pl;
+  v.Z = v.Y + v.s * (v.n1 + 1) * v.n2;
+  v.H = v.Z + v.s * v.n1 * (v.n2 + 1);
+  v.use_slot(0);
+  return v;
+}
+
+// write this slab's first plane into the lower neighbour's upper halo and its
+// last plane into the upper neighbour's lower halo, both in `slot`
+__device__ __forceinline__ void bc_push(const DLv& L, int slot, int rank, cooperative_groups::cluster_group& cl,
+                                        int tid) {
+  const int pl = L.n1 * L.n2;
+  if (rank > 0) {
+    float* dst = cl.map_shared_rank(L.H, rank - 1) + (2 * slot + 1) * pl;
+    for (int e = tid; e < pl; e += BC_NT) dst[e] = L.P[e];
+  }
+  if (rank < BC_CTAS - 1) {
+    float* dst = cl.map_shared_rank(L.H, rank + 1) + (2 * slot) * pl;
+    const float* src = L.P + (L.s - 1) * pl;
+    for (int e = tid; e < pl; e += BC_NT) dst[e] = src[e];
+  }
+}
+
+// b - A p at slab cell (li, j, k): k_bottom's restriction arithmetic, walls clamped
+__device__ __forceinline__ float bc_residual(const DLv& L, int li, int j, int k, int flux) {
+  const int n1 = L.n1, n2 = L.n2, sI = n1 * n2, i = L.i0 + li;
+  const int e = (li * n1 + j) * n2 + k, e2 = j * n2 + k;
+  const int fyi = (li * (n1 + 1) + j) * n2 + k, fzi = (li * n1 + j) * (n2 + 1) + k;
+  const float bxl = L.X[e], bxu = L.X[e + sI], byl = L.Y[fyi], byu = L.Y[fyi + n2], bzl = L.Z[fzi],
+              bzu = L.Z[fzi + 1];
+  const float* P = L.P;
+  const float pv = P[e];
+  const float q0 = li > 0 ? P[e - sI] : (i > 0 ? L.Plo[e2] : pv);
+  const float q1 = li < L.s - 1 ? P[e + sI] : (i < L.n0 - 1 ? L.Phi[e2] : pv);
+  const float q2 = P[j > 0 ? e - n2 : e], q3 = P[j < n1 - 1 ? e + n2 : e];
+  const float q4 = P[k > 0 ? e - 1 : e], q5 = P[k < n2 - 1 ? e + 1 : e];
+  float Ap;
+  if (flux) {
+    float sm = bxl * (pv - q0);
+    sm += bxu * (pv - q1);
+    sm += byl * (pv - q2);
+    sm += byu * (pv - q3);
+    sm += bzl * (pv - q4);
+    sm += bzu * (pv - q5);
+    Ap = sm;
+  } else {
+    const float d = bxl + bxu + byl + byu + bzl + bzu;
+    float sm = bxl * q0;
+    sm += bxu * q1;
+    sm += byl * q2;
+    sm += byu * q3;
+    sm += bzl * q4;
+    sm += bzu * q5;
+    Ap = d * pv - sm;
+  }
+  return L.B[e] - Ap;
+}
+
+// in-place relax of slab cell (li, j, k): bt_relax's arithmetic
+__device__ __forceinline__ void bc_relax(const DLv& L, int li, int j, int k, float omega, int flux) {
+  const int n1 = L.n1, n2 = L.n2, sI = n1 * n2, i = L.i0 + li;
+  const int e = (li * n1 + j) * n2 + k, e2 = j * n2 + k;
+  const int fyi = (li * (n1 + 1) + j) * n2 + k, fzi = (li * n1 + j) * (n2 + 1) + k;
+  const float bxl = L.X[e], bxu = L.X[e + sI], byl = L.Y[fyi], byu = L.Y[fyi + n2], bzl = L.Z[fzi],
+              bzu = L.Z[fzi + 1];
+  const float d = L.X[e] + L.X[e + sI] + L.Y[fyi] + L.Y[fyi + n2] + L.Z[fzi] + L.Z[fzi + 1];
+  if (!(d > 0.f)) return;
+  float* P = L.P;
+  const float pv = P[e];
+  const float q0 = li > 0 ? P[e - sI] : (i > 0 ? L.Plo[e2] : pv);
+  const float q1 = li < L.s - 1 ? P[e + sI] : (i < L.n0 - 1 ? L.Phi[e2] : pv);
+  const float q2 = P[j > 0 ? e - n2 : e], q3 = P[j < n1 - 1 ? e + n2 : e];
+  const float q4 = P[k > 0 ? e - 1 : e], q5 = P[k < n2 - 1 ? e + 1 : e];
+  float res;
+  if (flux) {
+    float sum = bxl * (pv - q0);
+    sum += bxu * (pv - q1);
+    sum += byl * (pv - q2);
+    sum += byu * (pv - q3);
+    sum += bzl * (pv - q4);
+    sum += bzu * (pv - q5);
+    res = L.B[e] - sum;
+  } else {
+    float sum = bxl * q0;
+    sum += bxu * q1;
+    sum += byl * q2;
+    sum += byu * q3;
+    sum += bzl * q4;
+    sum += bzu * q5;
+    res = L.B[e] - (d * pv - sum);
+  }
+  P[e] = pv + omega * res / d;
+}
+
+// the cells of `color` in this CTA's slab (n2 even: two cells per k pair);
+// shift indexing when n1 and n2 are powers of two
+__device__ __forceinline__ void bc_half_sweep(const DLv& L, int color, float omega, int flux, int tid) {
+  const int hk = L.n2 >> 1, hn = L.s * L.n1 * hk;
+  if (L.s1 >= 0 && L.s2 >= 1) {
+    const int sh = L.s2 - 1, hm = hk - 1, jm = L.n1 - 1;
+    for (int e = tid; e < hn; e += BC_NT) {
+      const int h = e & hm, row = e >> sh, j = row & jm, li = row >> L.s1;
+      const int k = 2 * h + ((color - (L.i0 + li) - j) & 1);
+      bc_relax(L, li, j, k, omega, flux);
+    }
+  } else {
+    for (int e = tid; e < hn; e += BC_NT) {
+      const int h = e % hk, row = e / hk, j = row % L.n1, li = row / L.n1;
+      const int k = 2 * h + ((color - (L.i0 + li) - j) & 1);
+      bc_relax(L, li, j, k, omega, flux);
+    }
+  }
+}
+
+// dst[e] = src[e] for e < n: FP32 arrays by 4-byte cp.async (completed by the
+// caller's cp.async.wait_all), 16-bit arrays widened through registers
+template <class S>
+__device__ __forceinline__ void bc_load(float* dst, const S* src, int n, int tid) {
+  if constexpr (std::is_same<S, float>::value) {
+    for (int e = tid; e < n; e += BC_NT)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst + e)),
+                   "l"(src + e)
+                   : "memory");
+  } else {
+    bt_load<S, BC_NT>(dst, src, n, 1.f, tid);
+  }
+}
+
+template <class T, class TB, class AccT>
+__global__ void __cluster_dims__(BC_CTAS, 1, 1) __launch_bounds__(BC_NT, 1) k_bottom_cluster(ClusterArgs<T, TB> a) {
+  if (is_done(a.st)) return;  // the flag is the same for every CTA of the launch
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char bcsm[];
+  __shared__ double sred[40];
+  __shared__ double s_mean;
+  __shared__ double s_part[BC_CTAS];
+  const int tid = threadIdx.x;
+  const int rank = (int)cl.block_rank();
+  const int nd = a.nd, nl = a.nl;
+  float* base = reinterpret_cast<float*>(bcsm);
+  float* lbase = base;  // after the slabs (the layout is the same in every CTA)
+  for (int l = 0; l < nd; ++l) lbase += bc_level_floats(a.D[l].n0, a.D[l].n1, a.D[l].n2);
+  auto align16 = [](float* p) {
+    return reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
+  };
+  // dense bottom: the full right-hand side of the level below, this CTA's rows
+  // of its solution and the partial sums of the product; otherwise CTA 0's
+  // levels and the coarsest solution
+  const bool dense = a.M != nullptr;
+  float* bfull = align16(lbase);
+  float* pd = align16(bfull + a.nb);
+  float* red = align16(pd + a.nb / BC_CTAS);
+  AccT* Pc;
+  {
+    float* end = lbase;
+    for (int l = 0; l < nl; ++l) end += bottom_level_floats(a.L[l].n0, a.L[l].n1, a.L[l].n2);
+    Pc = reinterpret_cast<AccT*>((reinterpret_cast<uintptr_t>(end) + 15) & ~uintptr_t(15));
+  }
   const float om = a.omega;
-  // ---- down: pre-smoothing, residual, restriction
-  for (int l = 0; l < nl - 1; ++l) {
-    const BottomLevel& L = a.L[l];
-    const LvPtr q = ptrs(l);
+
+  // ---- load: this CTA's slab of every distributed level, b of the top one;
+  // CTA 0 also the faces of its own levels; every P (and B below the top) zero
+  for (int l = 0; l < nd; ++l) {
+    const BottomLevel& G = a.D[l];
+    const DLv L = bc_level(a.D, base, l, rank, cl);
+    const int pl = G.n1 * G.n2;
+    bc_load(L.X, reinterpret_cast<const T*>(G.bx) + (size_t)L.i0 * pl, (L.s + 1) * pl, tid);
+    bc_load(L.Y, reinterpret_cast<const T*>(G.by) + (size_t)L.i0 * (G.n1 + 1) * G.n2, L.s * (G.n1 + 1) * G.n2, tid);
+    bc_load(L.Z, reinterpret_cast<const T*>(G.bz) + (size_t)L.i0 * G.n1 * (G.n2 + 1), L.s * G.n1 * (G.n2 + 1), tid);
+    for (int e = tid; e < L.s * pl; e += BC_NT) {
+      L.P[e] = 0.f;
+      if (l > 0) L.B[e] = 0.f;
+    }
+    for (int e = tid; e < 4 * pl; e += BC_NT) L.H[e] = 0.f;
+  }
+  {
+    const DLv L = bc_level(a.D, base, 0, rank, cl);
+    const int cnt = L.s * L.n1 * L.n2;
+    const TB* src = a.b + (size_t)L.i0 * L.n1 * L.n2;
+    if (a.b_scale) bt_load<TB, BC_NT>(L.B, src, cnt, *a.b_scale, tid);
+    else bc_load(L.B, src, cnt, tid);
+  }
+  if (rank == 0 && !dense) {
+    for (int l = 0; l < nl; ++l) {
+      const BottomLevel& G = a.L[l];
+      const BtPtrs q = bt_ptrs(a.L, lbase, l);
+      const int n = G.n0 * G.n1 * G.n2;
+      bc_load(q.X, reinterpret_cast<const T*>(G.bx), (G.n0 + 1) * G.n1 * G.n2, tid);
+      bc_load(q.Y, reinterpret_cast<const T*>(G.by), G.n0 * (G.n1 + 1) * G.n2, tid);
+      bc_load(q.Z, reinterpret_cast<const T*>(G.bz), G.n0 * G.n1 * (G.n2 + 1), tid);
+      for (int e = tid; e < n; e += BC_NT) q.P[e] = q.B[e] = 0.f;
+    }
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  cl.sync();
+
+  // ---- down the distributed levels: pre-smoothing, residual, restriction
+  int cur[BC_MAX_DIST];  // halo slot holding each level's current boundary planes
+  for (int l = 0; l < nd; ++l) {
+    DLv L = bc_level(a.D, base, l, rank, cl);
+    cur[l] = 0;
     for (int sw = 0; sw < a.pre; ++sw)
       for (int cc = 0; cc < 2; ++cc) {
-        bt_half_sweep<float>(L, q.P, q.B, q.X, q.Y, q.Z, cc, om, a.flux, tid, BT_NT);
-        __syncthreads();
+        L.use_slot(cur[l]);
+        bc_half_sweep(L, cc, om, a.flux, tid);
+        __syncthreads();  // the slab's half-sweep done before its boundary planes go out
+        cur[l] ^= 1;
+        bc_push(L, cur[l], rank, cl, tid);
+        cl.sync();
       }
-    const int n0 = L.n0, n1 = L.n1, n2 = L.n2;
-    const int C1 = n1 >> 1, C2 = n2 >> 1, nc = (n0 >> 1) * C1 * C2;
-    float* Bc = ptrs(l + 1).B;
-    const int sI = n1 * n2;
+    L.use_slot(cur[l]);
+    // coarse planes rank*s/2 .. : into the next slab, or into CTA 0's first
+    // level, or (dense) into every CTA's copy of the full right-hand side
+    const int C1 = L.n1 >> 1, C2 = L.n2 >> 1, hs = L.s >> 1, nc = hs * C1 * C2;
+    const bool last = l + 1 == nd;
+    float* Bc = !last ? bc_level(a.D, base, l + 1, rank, cl).B
+                      : dense ? bfull + (size_t)rank * nc : cl.map_shared_rank(bt_ptrs(a.L, lbase, 0).B, 0) + (size_t)rank * nc;
     const bool p2 = L.s1 >= 1 && L.s2 >= 1;
-    for (int ec = tid; ec < nc; ec += BT_NT) {
+    for (int ec = tid; ec < nc; ec += BC_NT) {
       int I, J, K;
       if (p2) {
         K = ec & (C2 - 1);
@@ -1214,105 +1666,163 @@ __global__ void __launch_bounds__(BT_NT) k_bottom(BottomArgs<T, TB> a) {
 #pragma unroll
         for (int bb = 0; bb < 2; ++bb)
 #pragma unroll
-          for (int cc = 0; cc < 2; ++cc) {
-            const int i = 2 * I + aa, j = 2 * J + bb, k = 2 * K + cc;
-            const int e = (i * n1 + j) * n2 + k;
-            const int fyi = (i * (n1 + 1) + j) * n2 + k, fzi = (i * n1 + j) * (n2 + 1) + k;
-            const float bxl = q.X[e], bxu = q.X[e + sI], byl = q.Y[fyi], byu = q.Y[fyi + n2], bzl = q.Z[fzi],
-                        bzu = q.Z[fzi + 1];
-            const float pv = q.P[e];
-            const float q0 = q.P[i > 0 ? e - sI : e], q1 = q.P[i < n0 - 1 ? e + sI : e];
-            const float q2 = q.P[j > 0 ? e - n2 : e], q3 = q.P[j < n1 - 1 ? e + n2 : e];
-            const float q4 = q.P[k > 0 ? e - 1 : e], q5 = q.P[k < n2 - 1 ? e + 1 : e];
-            float Ap;
-            if (a.flux) {
-              float sm = bxl * (pv - q0);
-              sm += bxu * (pv - q1);
-              sm += byl * (pv - q2);
-              sm += byu * (pv - q3);
-              sm += bzl * (pv - q4);
-              sm += bzu * (pv - q5);
-              Ap = sm;
-            } else {
-              const float d = bxl + bxu + byl + byu + bzl + bzu;
-              float sm = bxl * q0;
-              sm += bxu * q1;
-              sm += byl * q2;
-              sm += byu * q3;
-              sm += bzl * q4;
-              sm += bzu * q5;
-              Ap = d * pv - sm;
-            }
-            acc += q.B[e] - Ap;
-          }
-      Bc[ec] = roundT<T>(acc * a.rscale);
-    }
-    __syncthreads();
-  }
-  // ---- coarsest: sweeps from zero in AccT, then mean removal
-  {
-    const BottomLevel& L = a.L[nl - 1];
-    const LvPtr q = ptrs(nl - 1);
-    const int n = L.n0 * L.n1 * L.n2;
-    for (int e = tid; e < n; e += BT_NT) Pc[e] = AccT(0);
-    __syncthreads();
-    const bool one_warp = n <= 256;
-    const AccT omc = (AccT)om;
-    if (n <= 64 && (L.n2 & 1) == 0) {
-      if (tid < 32) bt_coarsest_regs<AccT>(L, Pc, q.B, q.X, q.Y, q.Z, omc, a.coarsest, a.flux, tid);
-    } else if (!one_warp || tid < 32) {
-      const int nt = one_warp ? 32 : BT_NT;
-      for (int sw = 0; sw < a.coarsest; ++sw) {
-        for (int color = 0; color < 2; ++color) {
-          bt_half_sweep<AccT>(L, Pc, q.B, q.X, q.Y, q.Z, color, omc, a.flux, tid, nt);
-          if (one_warp) __syncwarp();
-          else __syncthreads();
-        }
+          for (int c2 = 0; c2 < 2; ++c2) acc += bc_residual(L, 2 * I + aa, 2 * J + bb, 2 * K + c2, a.flux);
+      const float v = roundT<T>(acc * a.rscale);
+      if (last && dense) {
+        for (int r = 0; r < BC_CTAS; ++r) cl.map_shared_rank(Bc, r)[ec] = v;
+      } else {
+        Bc[ec] = v;
       }
     }
-    __syncthreads();
-    double ls = 0.0;
-    for (int e = tid; e < n; e += BT_NT) ls += (double)Pc[e];
-    const double tot = block_sum<BT_NT>(ls, sred);
-    if (tid == 0) s_mean = tot / (double)n;
-    __syncthreads();
-    const AccT shift = (AccT)(-s_mean);
-    for (int e = tid; e < n; e += BT_NT) q.P[e] = roundT<T>((float)(Pc[e] + shift));
-    __syncthreads();
+    cl.sync();
   }
-  // ---- up: prolongation, post-smoothing with the colours reversed
-  for (int l = nl - 2; l >= 0; --l) {
-    const BottomLevel& L = a.L[l];
-    const LvPtr q = ptrs(l);
-    const float* Pcoarse = ptrs(l + 1).P;
-    const int n = L.n0 * L.n1 * L.n2, h1 = L.n1 >> 1, h2 = L.n2 >> 1;
-    for (int e = tid; e < n; e += BT_NT) {
-      int i, j, k;
-      bt_ijk(L, e, i, j, k);
-      q.P[e] += Pcoarse[((i >> 1) * h1 + (j >> 1)) * h2 + (k >> 1)] * a.pscale;
+
+  // ---- the levels below: the dense operator's rows of this CTA's coarse
+  // planes (partial sums over column chunks, added in chunk order), or CTA 0
+  if (dense) {
+    const int nb = a.nb, R = nb / BC_CTAS, row0 = rank * R;
+    const int ch = R >= BC_NT ? 1 : BC_NT / R;  // column chunks per row
+    const int cw = (nb + ch - 1) / ch;
+    for (int t = tid; t < R * ch; t += BC_NT) {
+      const int i = t % R, c = t / R;
+      const int m0 = c * cw, m1 = min(nb, m0 + cw);
+      float acc = 0.f;
+      for (int m = m0; m < m1; ++m) acc = fmaf(__ldg(a.M + (size_t)m * nb + row0 + i), bfull[m], acc);
+      red[t] = acc;
     }
     __syncthreads();
+    for (int i = tid; i < R; i += BC_NT) {
+      float v = 0.f;
+      for (int c = 0; c < ch; ++c) v += red[c * R + i];
+      pd[i] = v;
+    }
+    __syncthreads();
+  } else {
+    if (rank == 0)
+      bt_local_vcycle<T, AccT, BC_NT>(a.L, lbase, 0, nl, Pc, om, a.pre, a.post, a.coarsest, a.rscale, a.pscale,
+                                      a.flux, sred, &s_mean);
+    cl.sync();
+  }
+
+  // ---- up the distributed levels: prolongation, post-smoothing with the colours reversed
+  for (int l = nd - 1; l >= 0; --l) {
+    DLv L = bc_level(a.D, base, l, rank, cl);
+    const int h1 = L.n1 >> 1, h2 = L.n2 >> 1, n = L.s * L.n1 * L.n2;
+    const float* Pcoarse;
+    int cplane0;  // global plane of Pcoarse's first plane
+    if (l + 1 < nd) {
+      Pcoarse = bc_level(a.D, base, l + 1, rank, cl).P;
+      cplane0 = L.i0 >> 1;
+    } else if (dense) {
+      Pcoarse = pd;
+      cplane0 = rank * (L.s >> 1);
+    } else {
+      Pcoarse = cl.map_shared_rank(bt_ptrs(a.L, lbase, 0).P, 0);
+      cplane0 = 0;
+    }
+    const bool p2 = L.s1 >= 0 && L.s2 >= 0;
+    for (int e = tid; e < n; e += BC_NT) {
+      int k, j, li;
+      if (p2) {
+        k = e & (L.n2 - 1);
+        const int t = e >> L.s2;
+        j = t & (L.n1 - 1);
+        li = t >> L.s1;
+      } else {
+        k = e % L.n2;
+        const int t = e / L.n2;
+        j = t % L.n1;
+        li = t / L.n1;
+      }
+      const int I = ((L.i0 + li) >> 1) - cplane0;
+      L.P[e] += Pcoarse[(I * h1 + (j >> 1)) * h2 + (k >> 1)] * a.pscale;
+    }
+    __syncthreads();  // the whole slab prolongated before its boundary planes go out
+    cur[l] ^= 1;
+    bc_push(L, cur[l], rank, cl, tid);
+    cl.sync();
     for (int sw = 0; sw < a.post; ++sw)
       for (int cc = 0; cc < 2; ++cc) {
-        bt_half_sweep<float>(L, q.P, q.B, q.X, q.Y, q.Z, 1 ^ cc, om, a.flux, tid, BT_NT);
+        L.use_slot(cur[l]);
+        bc_half_sweep(L, 1 ^ cc, om, a.flux, tid);
         __syncthreads();
+        cur[l] ^= 1;
+        bc_push(L, cur[l], rank, cl, tid);
+        cl.sync();
       }
   }
+
   // ---- output (and the mean when the top level is level 0)
-  const float* P0 = ptrs(0).P;
-  const int n = a.L[0].n0 * a.L[0].n1 * a.L[0].n2;
-  double ls = 0.0;
-  for (int e = tid; e < n; e += BT_NT) {
-    stT(a.p_out + e, P0[e]);
-    ls += (double)roundT<T>(P0[e]);
-  }
-  if (a.want_mean) {
-    const double tot = block_sum<BT_NT>(ls, sred);
-    if (tid == 0) {
-      a.st->sum_last = tot;
-      a.st->c_shift = (float)(-(tot / (double)n) * (a.mixed ? (double)a.st->zscale : 1.0));
+  {
+    const DLv L = bc_level(a.D, base, 0, rank, cl);
+    const int cnt = L.s * L.n1 * L.n2;
+    T* out = a.p_out + (size_t)L.i0 * L.n1 * L.n2;
+    double ls = 0.0;
+    for (int e = tid; e < cnt; e += BC_NT) {
+      stT(out + e, L.P[e]);
+      ls += (double)roundT<T>(L.P[e]);
+    }
+    if (a.want_mean) {
+      const double bs = block_sum<BC_NT>(ls, sred);
+      if (tid == 0) *cl.map_shared_rank(&s_part[rank], 0) = bs;
     }
   }
+  cl.sync();  // also: no CTA leaves while another may still read its shared memory
+  if (a.want_mean && rank == 0 && tid == 0) {
+    double tot = 0.0;
+    for (int r = 0; r < BC_CTAS; ++r) tot += s_part[r];
+    const int n = a.D[0].n0 * a.D[0].n1 * a.D[0].n2;
+    a.st->sum_last = tot;
+    a.st->c_shift = (float)(-(tot / (double)n) * (a.mixed ? (double)a.st->zscale : 1.0));
+  }
+}
+
+// ---- the dense bottom operator, one column per CTA: the V-cycle of the
+// levels below the cluster's slabs (bt_local_vcycle, DB_NT threads) applied to
+// the unit right-hand side e_m, written to M[m * nb + i]
+constexpr int DB_NT = 128;
+
+template <class T> struct DenseBuildArgs {
+  int nl;
+  BottomLevel L[PF_MG_MAX_LEVELS];
+  float* M;
+  float omega;
+  int pre, post, coarsest;
+  float rscale, pscale;
+  int flux;
+};
+
+template <class T, class AccT>
+__global__ void __launch_bounds__(DB_NT) k_bottom_dense_build(DenseBuildArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char dbsm[];
+  __shared__ double sred[40];
+  __shared__ double s_mean;
+  const int tid = threadIdx.x, m = blockIdx.x;
+  float* base = reinterpret_cast<float*>(dbsm);
+  AccT* Pc;
+  {
+    float* end = base;
+    for (int l = 0; l < a.nl; ++l) end += bottom_level_floats(a.L[l].n0, a.L[l].n1, a.L[l].n2);
+    Pc = reinterpret_cast<AccT*>((reinterpret_cast<uintptr_t>(end) + 15) & ~uintptr_t(15));
+  }
+  for (int l = 0; l < a.nl; ++l) {
+    const BottomLevel& G = a.L[l];
+    const BtPtrs q = bt_ptrs(a.L, base, l);
+    const int n = G.n0 * G.n1 * G.n2;
+    bt_load<T, DB_NT>(q.X, reinterpret_cast<const T*>(G.bx), (G.n0 + 1) * G.n1 * G.n2, 1.f, tid);
+    bt_load<T, DB_NT>(q.Y, reinterpret_cast<const T*>(G.by), G.n0 * (G.n1 + 1) * G.n2, 1.f, tid);
+    bt_load<T, DB_NT>(q.Z, reinterpret_cast<const T*>(G.bz), G.n0 * G.n1 * (G.n2 + 1), 1.f, tid);
+    for (int e = tid; e < n; e += DB_NT) {
+      q.P[e] = 0.f;
+      q.B[e] = (l == 0 && e == m) ? 1.f : 0.f;
+    }
+  }
+  __syncthreads();
+  bt_local_vcycle<T, AccT, DB_NT>(a.L, base, 0, a.nl, Pc, a.omega, a.pre, a.post, a.coarsest, a.rscale, a.pscale,
+                                  a.flux, sred, &s_mean);
+  const float* P0 = bt_ptrs(a.L, base, 0).P;
+  const int nb = a.L[0].n0 * a.L[0].n1 * a.L[0].n2;
+  for (int i = tid; i < nb; i += DB_NT) a.M[(size_t)m * nb + i] = P0[i];
 }
 
 // --------------------------------------------------------------- CG vector kernels
@@ -1667,6 +2177,10 @@ struct pf_mg_plan {
   int sms;             // multiprocessors of the plan's device (persistent sweep grid)
   size_t bottom_smem;  // dynamic shared memory of the bottom kernel
   bool bottom_stage;   // bottom_smem includes the 16-bit staging area
+  int bc_nd;           // > 0: levels lb .. lb+bc_nd-1 run distributed on a CTA cluster (k_bottom_cluster)
+  size_t bc_smem;      // dynamic shared memory per CTA of the cluster kernel
+  int dense_nb;        // > 0: the levels below the slabs run as a dense nb x nb operator in bottom_op
+  float* bottom_op;
   cudaStream_t cap_stream;
   cudaGraphExec_t exec[2];
   size_t exec_nodes[2];
@@ -1845,8 +2359,54 @@ int launch_sweep(pf_mg_plan* P, int lv, const T* p_in, bool zero_in, T* p_out, c
   return PF_OK;
 }
 
+int lg2_exact(int v) {
+  int s = 0;
+  while ((1 << s) < v) ++s;
+  return (1 << s) == v ? s : -1;
+}
+
+template <class T> BottomLevel bottom_level(pf_mg_plan* P, int lv) {
+  const pf_mg_level& L = P->d.lev[lv];
+  LV<T> V = view<T>(P, lv);
+  const int s1 = lg2_exact(L.ny), s2 = lg2_exact(L.nz);
+  const bool p2 = s1 >= 0 && s2 >= 0;
+  return BottomLevel{L.nx, L.ny, L.nz, p2 ? s1 : -1, p2 ? s2 : -1, V.bx, V.by, V.bz};
+}
+
+template <class T, class TB>
+int launch_bottom_cluster(pf_mg_plan* P, const TB* b, const float* b_scale, bool want_mean, cudaStream_t s, T** out) {
+  ClusterArgs<T, TB> a;
+  const int lb = P->lb, nlev = P->d.nlev;
+  a.nd = P->bc_nd;
+  for (int l = 0; l < a.nd; ++l) a.D[l] = bottom_level<T>(P, lb + l);
+  a.nl = nlev - lb - a.nd;
+  for (int l = 0; l < a.nl; ++l) a.L[l] = bottom_level<T>(P, lb + a.nd + l);
+  LV<T> V0 = view<T>(P, lb);
+  a.b = b;
+  a.b_scale = b_scale;
+  a.p_out = V0.p0;
+  a.omega = P->d.omega;
+  a.pre = P->d.pre;
+  a.post = P->d.post;
+  a.coarsest = P->d.coarsest;
+  a.rscale = mixed(P) ? 0.125f : 1.f;
+  a.pscale = mixed(P) ? 2.f : 1.f;
+  a.flux = FLUX(P);
+  a.st = ST(P);
+  a.want_mean = want_mean ? 1 : 0;
+  a.mixed = mixed(P) ? 1 : 0;
+  a.M = P->dense_nb ? P->bottom_op : nullptr;
+  a.nb = P->dense_nb;
+  if (mixed(P)) k_bottom_cluster<T, TB, double><<<BC_CTAS, BC_NT, P->bc_smem, s>>>(a);
+  else k_bottom_cluster<T, TB, float><<<BC_CTAS, BC_NT, P->bc_smem, s>>>(a);
+  PF_LAUNCHED();
+  *out = V0.p0;
+  return PF_OK;
+}
+
 template <class T, class TB>
 int launch_bottom(pf_mg_plan* P, const TB* b, const float* b_scale, bool want_mean, cudaStream_t s, T** out) {
+  if (P->bc_nd > 0) return launch_bottom_cluster<T, TB>(P, b, b_scale, want_mean, s, out);
   BottomArgs<T, TB> a;
   const int lb = P->lb;
   a.nl = P->d.nlev - lb;
@@ -2120,6 +2680,32 @@ int solve_impl(pf_mg_plan* P, const float* b, float* x, float tol, int max_iter,
   return PF_OK;
 }
 
+// the dense operator of the levels below the cluster's slabs, one column per CTA
+template <class T> int launch_dense_build(pf_mg_plan* P, cudaStream_t s) {
+  DenseBuildArgs<T> a;
+  const int l0 = P->lb + P->bc_nd;
+  a.nl = P->d.nlev - l0;
+  size_t floats = 0;
+  for (int l = 0; l < a.nl; ++l) {
+    a.L[l] = bottom_level<T>(P, l0 + l);
+    floats += bottom_level_floats(a.L[l].n0, a.L[l].n1, a.L[l].n2);
+  }
+  a.M = P->bottom_op;
+  a.omega = P->d.omega;
+  a.pre = P->d.pre;
+  a.post = P->d.post;
+  a.coarsest = P->d.coarsest;
+  a.rscale = mixed(P) ? 0.125f : 1.f;
+  a.pscale = mixed(P) ? 2.f : 1.f;
+  a.flux = FLUX(P);
+  const BottomLevel& Lc = a.L[a.nl - 1];
+  const size_t smem = floats * sizeof(float) + 16 + (size_t)Lc.n0 * Lc.n1 * Lc.n2 * sizeof(double);
+  if (mixed(P)) k_bottom_dense_build<T, double><<<P->dense_nb, DB_NT, smem, s>>>(a);
+  else k_bottom_dense_build<T, float><<<P->dense_nb, DB_NT, smem, s>>>(a);
+  PF_LAUNCHED();
+  return PF_OK;
+}
+
 template <class T> int build_impl(pf_mg_plan* P, cudaStream_t s) {
   for (int lv = 0; lv < P->d.nlev; ++lv) {
     const pf_mg_level& L = P->d.lev[lv];
@@ -2139,6 +2725,10 @@ template <class T> int build_impl(pf_mg_plan* P, cudaStream_t s) {
                                                     C.bz);
       PF_LAUNCHED();
     }
+  }
+  if (P->dense_nb) {
+    const int rc = launch_dense_build<T>(P, s);
+    if (rc != PF_OK) return rc;
   }
   return PF_OK;
 }
@@ -2168,6 +2758,12 @@ template <class T> cudaError_t set_smem_attrs() {
   chk(cudaFuncSetAttribute(k_bottom<T, T, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   chk(cudaFuncSetAttribute(k_bottom<T, float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   chk(cudaFuncSetAttribute(k_bottom<T, T, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  chk(cudaFuncSetAttribute(k_bottom_cluster<T, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  chk(cudaFuncSetAttribute(k_bottom_cluster<T, T, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  chk(cudaFuncSetAttribute(k_bottom_cluster<T, float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  chk(cudaFuncSetAttribute(k_bottom_cluster<T, T, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  chk(cudaFuncSetAttribute(k_bottom_dense_build<T, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  chk(cudaFuncSetAttribute(k_bottom_dense_build<T, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   chk(cudaFuncSetAttribute(k_rb_tile<T, float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile));
   chk(cudaFuncSetAttribute(k_rb_tile<T, T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile));
   chk(cudaFuncSetAttribute(k_rb_tile_tma<4, SW_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2187,6 +2783,94 @@ template <class T> cudaError_t set_smem_attrs() {
 }
 
 }  // namespace
+
+struct BottomSel {
+  int lb = 0;              // first level of the bottom kernel
+  size_t bottom_smem = 0;  // single-CTA kernel
+  bool bottom_stage = false;
+  int bc_nd = 0;           // cluster kernel: distributed levels
+  size_t bc_smem = 0;
+  int dense_nb = 0;        // dense operator of the levels below the slabs: its size (cells)
+  size_t bc_smem_dense = 0;
+};
+
+// The bottom of a plan's V-cycle (pf_mg_plan_create, pf_mg_bottom_op_floats).
+BottomSel select_bottom(const pf_mg_desc* desc) {
+  BottomSel r;
+  // bottom kernel: the deepest run of levels that each fit kBottomMaxCells and
+  // together fit the shared memory of one CTA
+  r.lb = desc->nlev;
+  r.bottom_smem = 0;
+  r.bottom_stage = desc->precision != PF_PREC_FP32;
+  {
+    // 16-bit hierarchy: a staging area for the raw 16-bit faces (and b, at
+    // most 4 bytes a cell) behind the coarsest solution
+    size_t floats = 0, faces = 0;
+    const pf_mg_level& Lc = desc->lev[desc->nlev - 1];
+    for (int lv = desc->nlev - 1; lv >= 0; --lv) {
+      const pf_mg_level& L = desc->lev[lv];
+      const long long n = (long long)L.nx * L.ny * L.nz;
+      const size_t f2 = floats + bottom_level_floats(L.nx, L.ny, L.nz);
+      const size_t fc2 = faces + bottom_level_floats(L.nx, L.ny, L.nz) - 2 * (size_t)n;
+      const size_t stage = r.bottom_stage ? 16 + 2 * fc2 + 4 * (size_t)n : 0;
+      const size_t bytes = f2 * sizeof(float) + 16 + (size_t)Lc.nx * Lc.ny * Lc.nz * sizeof(double) + stage;
+      if (n > kBottomMaxCells || bytes > 200 * 1024) break;
+      floats = f2;
+      faces = fc2;
+      r.lb = lv;
+      r.bottom_smem = bytes;
+    }
+  }
+  // cluster bottom (k_bottom_cluster): the finest start level lv < lb such
+  // that lv .. lv+nd-1 halve exactly and split into even slabs over BC_CTAS
+  // CTAs (n0 a multiple of 2*BC_CTAS, n1 and n2 even), at least one level is
+  // left for CTA 0, and slabs, CTA 0's levels and the FP64 coarsest fit one
+  // CTA's shared memory.  PFFLIP_MG_BOTTOM=cta keeps the single-CTA bottom.
+  r.bc_nd = 0;
+  r.bc_smem = 0;
+  {
+    const char* env = std::getenv("PFFLIP_MG_BOTTOM");
+    const bool allow = !(env && std::strcmp(env, "cta") == 0);
+    const bool allow_dense = !(env && (std::strcmp(env, "cta") == 0 || std::strcmp(env, "cluster") == 0));
+    const int nlev = desc->nlev;
+    const pf_mg_level& Lc = desc->lev[nlev - 1];
+    for (int lv = 0; allow && lv < r.lb; ++lv) {
+      auto halves = [&](int l) {
+        const pf_mg_level& F = desc->lev[l];
+        const pf_mg_level& C = desc->lev[l + 1];
+        return C.nx * 2 == F.nx && C.ny * 2 == F.ny && C.nz * 2 == F.nz;
+      };
+      int nd = 0;
+      size_t floats = 0;
+      while (lv + nd < nlev - 1 && nd < BC_MAX_DIST) {
+        const pf_mg_level& L = desc->lev[lv + nd];
+        if (L.nx % (2 * BC_CTAS) != 0 || L.ny % 2 != 0 || L.nz % 2 != 0 || !halves(lv + nd)) break;
+        floats += bc_level_floats(L.nx, L.ny, L.nz);
+        ++nd;
+      }
+      if (nd == 0) continue;
+      for (int l = lv + nd; l < nlev; ++l)
+        floats += bottom_level_floats(desc->lev[l].nx, desc->lev[l].ny, desc->lev[l].nz);
+      const size_t bytes = floats * sizeof(float) + 16 + (size_t)Lc.nx * Lc.ny * Lc.nz * sizeof(double);
+      if (bytes > 200 * 1024) continue;
+      r.bc_nd = nd;
+      r.bc_smem = bytes;
+      r.lb = lv;
+      // dense bottom: the levels below the slabs as one operator on the first of
+      // them, each CTA applying the rows of its own coarse planes
+      const pf_mg_level& F = desc->lev[lv + nd];
+      const int nb = F.nx * F.ny * F.nz;
+      if (allow_dense && nb <= kDenseMaxCells && F.nx % BC_CTAS == 0) {
+        size_t dfl = 0;
+        for (int l = lv; l < lv + nd; ++l) dfl += bc_level_floats(desc->lev[l].nx, desc->lev[l].ny, desc->lev[l].nz);
+        r.dense_nb = nb;
+        r.bc_smem_dense = (dfl + 4 + (size_t)nb + 4 + (size_t)(nb / BC_CTAS) + 4 + BC_NT) * sizeof(float);
+      }
+      break;
+    }
+  }
+  return r;
+}
 
 extern "C" {
 
@@ -2245,29 +2929,16 @@ int pf_mg_plan_create(const pf_mg_desc* desc, pf_mg_plan** out) {
     const pf_mg_level& L = desc->lev[lv];
     P->lp_scale[lv] = std::ldexp(desc->coef_scale > 0.f ? desc->coef_scale : 1.f, -2 * lv);
   }
-  // bottom kernel: the deepest run of levels that each fit kBottomMaxCells and
-  // together fit the shared memory of one CTA
-  P->lb = desc->nlev;
-  P->bottom_smem = 0;
-  P->bottom_stage = desc->precision != PF_PREC_FP32;
   {
-    // 16-bit hierarchy: a staging area for the raw 16-bit faces (and b, at
-    // most 4 bytes a cell) behind the coarsest solution
-    size_t floats = 0, faces = 0;
-    const pf_mg_level& Lc = desc->lev[desc->nlev - 1];
-    for (int lv = desc->nlev - 1; lv >= 0; --lv) {
-      const pf_mg_level& L = desc->lev[lv];
-      const long long n = (long long)L.nx * L.ny * L.nz;
-      const size_t f2 = floats + bottom_level_floats(L.nx, L.ny, L.nz);
-      const size_t fc2 = faces + bottom_level_floats(L.nx, L.ny, L.nz) - 2 * (size_t)n;
-      const size_t stage = P->bottom_stage ? 16 + 2 * fc2 + 4 * (size_t)n : 0;
-      const size_t bytes = f2 * sizeof(float) + 16 + (size_t)Lc.nx * Lc.ny * Lc.nz * sizeof(double) + stage;
-      if (n > kBottomMaxCells || bytes > 200 * 1024) break;
-      floats = f2;
-      faces = fc2;
-      P->lb = lv;
-      P->bottom_smem = bytes;
-    }
+    const BottomSel sel = select_bottom(desc);
+    P->lb = sel.lb;
+    P->bottom_smem = sel.bottom_smem;
+    P->bottom_stage = sel.bottom_stage;
+    P->bc_nd = sel.bc_nd;
+    P->bc_smem = sel.bc_smem;
+    P->dense_nb = (sel.dense_nb > 0 && desc->bottom_op) ? sel.dense_nb : 0;
+    if (P->dense_nb) P->bc_smem = sel.bc_smem_dense;
+    P->bottom_op = desc->bottom_op;
   }
   cudaError_t e = cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&P->h_state[0], sizeof(pf::MGState) * 2, cudaHostAllocDefault);
@@ -2303,6 +2974,20 @@ int pf_mg_plan_destroy(pf_mg_plan* P) {
   if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
   delete P;
   return PF_OK;
+}
+
+int pf_mg_bottom_info(const pf_mg_plan* P, int32_t* first_level, int32_t* cluster_levels, int32_t* dense) {
+  PF_REQUIRE(P && first_level && cluster_levels && dense, "null argument");
+  *first_level = P->lb;
+  *cluster_levels = P->bc_nd;
+  *dense = P->dense_nb > 0 ? 1 : 0;
+  return PF_OK;
+}
+
+int64_t pf_mg_bottom_op_floats(const pf_mg_desc* desc) {
+  if (!desc || desc->nlev < 1 || desc->nlev > PF_MG_MAX_LEVELS) return 0;
+  const BottomSel sel = select_bottom(desc);
+  return sel.dense_nb > 0 ? (int64_t)sel.dense_nb * sel.dense_nb : 0;
 }
 
 int pf_mg_build_hierarchy(pf_mg_plan* P, const float* bx, const float* by, const float* bz, void* stream) {

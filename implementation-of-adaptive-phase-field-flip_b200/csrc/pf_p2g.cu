@@ -17,8 +17,10 @@
 // fx = (n + o)*dx - x in the reference's order (d^2/r^2 as d^2*(1/r^2)).  The
 // register box includes nodes outside the reference's window
 // floor(c - R) + 1 .. floor(c + R); those lie at least r away, so their
-// weight is exactly 0, and nodes outside the grid are never flushed.
+// weight is exactly 0, and nodes outside the grid are never flushed.  The
+// weight arithmetic runs on packed f32x2 pairs.
 #include "pf_common.cuh"
+#include "pf_f32x2.cuh"
 
 namespace pf {
 
@@ -40,55 +42,118 @@ struct P2GArgs {
 };
 
 // Register box of grid G (0,1,2 = face axis, 3 = cell centres) for one cell.
+// The accumulators are packed pairs (f32x2) along one axis PA: the face
+// grids pair their two nodes along the normal axis, the cell grid pairs z
+// nodes 0 and 1 and keeps z node 2 in scalars.  Every node still sums its
+// particles in particle order with the scalar operations
+// d^2 = (dx^2 + dy^2) + dz^2, t = max(fma(-d^2, 1/r^2, 1), 0), w = (t t) t,
+// wm = w m_p, m += wm, q += wm u (fma) or q += w.
 template <int G> struct Box {
   static constexpr int NX = (G == 0) ? 2 : 3, NY = (G == 1) ? 2 : 3, NZ = (G == 2) ? 2 : 3;
   static constexpr int LX = (G == 0) ? 0 : -1, LY = (G == 1) ? 0 : -1, LZ = (G == 2) ? 0 : -1;
   static constexpr float OX = (G == 0) ? 0.f : 0.5f, OY = (G == 1) ? 0.f : 0.5f, OZ = (G == 2) ? 0.f : 0.5f;
-  float m[NX][NY][NZ];   // sum of w * m_p
-  float q[NX][NY][NZ];   // sum of w * m_p * u_G (faces) or of w (cells)
+  static constexpr int PA = G < 3 ? G : 2;  // paired axis
+  static constexpr int QX = PA == 0 ? 1 : NX, QY = PA == 1 ? 1 : NY, QZ = PA == 2 ? 1 : NZ;
+  static constexpr int SX = G == 3 ? 3 : 1;  // cell grid: scalar z node 2 per (a, b)
+  f2 m2[QX][QY][QZ];  // sum of w * m_p
+  f2 q2[QX][QY][QZ];  // sum of w * m_p * u_G (faces) or of w (cells)
+  float m1[SX][SX], q1[SX][SX];
 
   __device__ __forceinline__ void zero() {
+    const f2 z = f2_bcast(0.f);
 #pragma unroll
-    for (int a = 0; a < NX; ++a)
+    for (int a = 0; a < QX; ++a)
 #pragma unroll
-      for (int b = 0; b < NY; ++b)
+      for (int b = 0; b < QY; ++b)
 #pragma unroll
-        for (int c = 0; c < NZ; ++c) m[a][b][c] = q[a][b][c] = 0.f;
+        for (int c = 0; c < QZ; ++c) m2[a][b][c] = q2[a][b][c] = z;
+#pragma unroll
+    for (int a = 0; a < SX; ++a)
+#pragma unroll
+      for (int b = 0; b < SX; ++b) m1[a][b] = q1[a][b] = 0.f;
+  }
+
+  // the accumulated values of node (a, b, c)
+  __device__ __forceinline__ float M(int a, int b, int c) const {
+    if (G == 3 && c == 2) return m1[a][b];
+    const f2 v = m2[PA == 0 ? 0 : a][PA == 1 ? 0 : b][PA == 2 ? 0 : c];
+    return (PA == 0 ? a : PA == 1 ? b : c) == 0 ? f2_x(v) : f2_y(v);
+  }
+  __device__ __forceinline__ float Q(int a, int b, int c) const {
+    if (G == 3 && c == 2) return q1[a][b];
+    const f2 v = q2[PA == 0 ? 0 : a][PA == 1 ? 0 : b][PA == 2 ? 0 : c];
+    return (PA == 0 ? a : PA == 1 ? b : c) == 0 ? f2_x(v) : f2_y(v);
+  }
+
+  __device__ __forceinline__ void node2(f2 s2, f2 ninv, f2 one, f2 mp2, f2 up2, f2& m, f2& q) {
+    const f2 t = f2_relu(f2_fma(s2, ninv, one));
+    const f2 w = f2_mul(f2_mul(t, t), t);
+    const f2 wm = f2_mul(w, mp2);
+    m = f2_add(m, wm);
+    q = (G < 3) ? f2_fma(wm, up2, q) : f2_add(q, w);
+  }
+
+  // squared distances along one axis to the nodes c + L + o: a pair (o = 0, 1)
+  // for the paired axis, broadcast pairs per node otherwise
+  template <int N, int L, bool PAIRED>
+  __device__ __forceinline__ static void dist2(int c, float off, float x, f2 dx2, f2* out) {
+    const f2 gx = f2_bcast(-x);
+    if (PAIRED) {
+      const f2 f = f2_fma(f2_make((float)(c + L) + off, (float)(c + L + 1) + off), dx2, gx);
+      out[0] = f2_mul(f, f);
+    } else {
+#pragma unroll
+      for (int o = 0; o < N; ++o) {
+        const f2 f = f2_fma(f2_bcast((float)(c + L + o) + off), dx2, gx);
+        out[o] = f2_mul(f, f);
+      }
+    }
   }
 
   // add one particle (x, mass, velocity component) of cell (ci, cj, ck)
   __device__ __forceinline__ void add(int ci, int cj, int ck, const float x[3], float mp, float up, float dx,
                                       float inv_r2) {
-    float DX[NX], DY[NY], DZ[NZ];
-#pragma unroll
-    for (int a = 0; a < NX; ++a) {
-      const float f = ((float)(ci + LX + a) + OX) * dx - x[0];
-      DX[a] = f * f;
+    const f2 dx2 = f2_bcast(dx), ninv = f2_bcast(-inv_r2), one = f2_bcast(1.f);
+    const f2 mp2 = f2_bcast(mp), up2 = f2_bcast(up);
+    f2 DX[PA == 0 ? 1 : NX], DY[PA == 1 ? 1 : NY], DZ[PA == 2 ? 1 : NZ];
+    dist2<NX, LX, PA == 0>(ci, OX, x[0], dx2, DX);
+    dist2<NY, LY, PA == 1>(cj, OY, x[1], dx2, DY);
+    dist2<NZ, LZ, PA == 2>(ck, OZ, x[2], dx2, DZ);
+    float dz2 = 0.f;  // cell grid: z node 2
+    if (G == 3) {
+      const float f = fmaf((float)(ck + LZ + 2) + OZ, dx, -x[2]);
+      dz2 = f * f;
     }
-#pragma unroll
-    for (int b = 0; b < NY; ++b) {
-      const float f = ((float)(cj + LY + b) + OY) * dx - x[1];
-      DY[b] = f * f;
-    }
-#pragma unroll
-    for (int c = 0; c < NZ; ++c) {
-      const float f = ((float)(ck + LZ + c) + OZ) * dx - x[2];
-      DZ[c] = f * f;
-    }
-#pragma unroll
-    for (int a = 0; a < NX; ++a)
+    if (PA == 0) {
 #pragma unroll
       for (int b = 0; b < NY; ++b) {
-        const float dxy = DX[a] + DY[b];
+        const f2 dxy = f2_add(DX[0], DY[b]);
 #pragma unroll
-        for (int c = 0; c < NZ; ++c) {
-          const float t = fmaxf(1.f - (dxy + DZ[c]) * inv_r2, 0.f);
-          const float w = t * t * t;
-          const float wm = w * mp;
-          m[a][b][c] += wm;
-          q[a][b][c] += (G < 3) ? wm * up : w;
-        }
+        for (int c = 0; c < NZ; ++c) node2(f2_add(dxy, DZ[c]), ninv, one, mp2, up2, m2[0][b][c], q2[0][b][c]);
       }
+    } else if (PA == 1) {
+#pragma unroll
+      for (int a = 0; a < NX; ++a) {
+        const f2 dxy = f2_add(DX[a], DY[0]);
+#pragma unroll
+        for (int c = 0; c < NZ; ++c) node2(f2_add(dxy, DZ[c]), ninv, one, mp2, up2, m2[a][0][c], q2[a][0][c]);
+      }
+    } else {
+#pragma unroll
+      for (int a = 0; a < NX; ++a)
+#pragma unroll
+        for (int b = 0; b < NY; ++b) {
+          const f2 dxy = f2_add(DX[a], DY[b]);
+          node2(f2_add(dxy, DZ[0]), ninv, one, mp2, up2, m2[a][b][0], q2[a][b][0]);
+          if (G == 3) {
+            const float t = fmaxf(fmaf(f2_x(dxy) + dz2, -inv_r2, 1.f), 0.f);
+            const float w = t * t * t;
+            const float wm = w * mp;
+            m1[a < SX ? a : 0][b < SX ? b : 0] += wm;
+            q1[a < SX ? a : 0][b < SX ? b : 0] += w;
+          }
+        }
+    }
   }
 
   // combine along k across the lanes of the row and add to the shared boxes.
@@ -101,34 +166,34 @@ template <int G> struct Box {
         const int row = ((li + a) * PG_BJ + (lj + b)) * PG_BK;
         if (NZ == 3) {
           // node k0+l (box index l+1) = own centre + lane l-1's upper + lane l+1's lower
-          const float up1 = __shfl_up_sync(0xffffffffu, m[a][b][2], 1);
-          const float up2 = __shfl_up_sync(0xffffffffu, q[a][b][2], 1);
-          const float dn1 = __shfl_down_sync(0xffffffffu, m[a][b][0], 1);
-          const float dn2 = __shfl_down_sync(0xffffffffu, q[a][b][0], 1);
-          float v1 = m[a][b][1], v2 = q[a][b][1];
+          const float up1 = __shfl_up_sync(0xffffffffu, M(a, b, 2), 1);
+          const float up2 = __shfl_up_sync(0xffffffffu, Q(a, b, 2), 1);
+          const float dn1 = __shfl_down_sync(0xffffffffu, M(a, b, 0), 1);
+          const float dn2 = __shfl_down_sync(0xffffffffu, Q(a, b, 0), 1);
+          float v1 = M(a, b, 1), v2 = Q(a, b, 1);
           if (lane > 0) { v1 += up1; v2 += up2; }
           if (lane < 31) { v1 += dn1; v2 += dn2; }
           if (v1 != 0.f) atomicAdd(sm1 + row + lane + 1, v1);
           if (v2 != 0.f) atomicAdd(sm2 + row + lane + 1, v2);
           if (lane == 0) {
-            if (m[a][b][0] != 0.f) atomicAdd(sm1 + row, m[a][b][0]);
-            if (q[a][b][0] != 0.f) atomicAdd(sm2 + row, q[a][b][0]);
+            if (M(a, b, 0) != 0.f) atomicAdd(sm1 + row, M(a, b, 0));
+            if (Q(a, b, 0) != 0.f) atomicAdd(sm2 + row, Q(a, b, 0));
           }
           if (lane == 31) {
-            if (m[a][b][2] != 0.f) atomicAdd(sm1 + row + 33, m[a][b][2]);
-            if (q[a][b][2] != 0.f) atomicAdd(sm2 + row + 33, q[a][b][2]);
+            if (M(a, b, 2) != 0.f) atomicAdd(sm1 + row + 33, M(a, b, 2));
+            if (Q(a, b, 2) != 0.f) atomicAdd(sm2 + row + 33, Q(a, b, 2));
           }
         } else {
           // z-faces: node k0+l (box index l) = own lower + lane l-1's upper
-          const float up1 = __shfl_up_sync(0xffffffffu, m[a][b][NZ - 1], 1);
-          const float up2 = __shfl_up_sync(0xffffffffu, q[a][b][NZ - 1], 1);
-          float v1 = m[a][b][0], v2 = q[a][b][0];
+          const float up1 = __shfl_up_sync(0xffffffffu, M(a, b, NZ - 1), 1);
+          const float up2 = __shfl_up_sync(0xffffffffu, Q(a, b, NZ - 1), 1);
+          float v1 = M(a, b, 0), v2 = Q(a, b, 0);
           if (lane > 0) { v1 += up1; v2 += up2; }
           if (v1 != 0.f) atomicAdd(sm1 + row + lane, v1);
           if (v2 != 0.f) atomicAdd(sm2 + row + lane, v2);
           if (lane == 31) {
-            if (m[a][b][NZ - 1] != 0.f) atomicAdd(sm1 + row + 32, m[a][b][NZ - 1]);
-            if (q[a][b][NZ - 1] != 0.f) atomicAdd(sm2 + row + 32, q[a][b][NZ - 1]);
+            if (M(a, b, NZ - 1) != 0.f) atomicAdd(sm1 + row + 32, M(a, b, NZ - 1));
+            if (Q(a, b, NZ - 1) != 0.f) atomicAdd(sm2 + row + 32, Q(a, b, NZ - 1));
           }
         }
       }

@@ -67,6 +67,7 @@ class pf_mg_desc(C.Structure):
         ("rhs", C.c_void_p), ("res_v", C.c_void_p), ("res_alt", C.c_void_p), ("z", C.c_void_p),
         ("q", C.c_void_p), ("Ap", C.c_void_p), ("x", C.c_void_p),
         ("state", C.c_void_p), ("partials", C.c_void_p), ("counters", C.c_void_p),
+        ("bottom_op", C.c_void_p),
     ]
 
 
@@ -109,6 +110,8 @@ SIGNATURES = {
     "pf_mg_level_count": (C.c_int32, [_I32, _I32, _I32, _I32, C.POINTER(_I32)]),
     "pf_mg_plan_create": (C.c_int, [C.POINTER(pf_mg_desc), C.POINTER(_VP)]),
     "pf_mg_plan_destroy": (C.c_int, [_VP]),
+    "pf_mg_bottom_info": (C.c_int, [_VP, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(_I32)]),
+    "pf_mg_bottom_op_floats": (C.c_int64, [C.POINTER(pf_mg_desc)]),
     "pf_mg_build_hierarchy": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "pf_mg_precondition": (C.c_int, [_VP, _VP, _VP, _VP]),
     "pf_mg_smooth": (C.c_int, [_VP, _I32, _I32, _I32, _VP]),

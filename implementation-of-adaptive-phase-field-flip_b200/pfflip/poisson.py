@@ -130,6 +130,9 @@ class MGPCG:
         d.rhs, d.res_v, d.res_alt, d.z = N.ptr(self.rhs), N.ptr(self.res_v), N.ptr(self.r_prev), N.ptr(self.z)
         d.q, d.Ap, d.x = N.ptr(self.q), N.ptr(self.Ap), N.ptr(self.x)
         d.state, d.partials, d.counters = self._state.data_ptr(), self._partials.data_ptr(), self._counters.data_ptr()
+        nop = int(N.lib().pf_mg_bottom_op_floats(C.byref(d)))  # dense operator of the smallest levels (or 0)
+        self._bottom_op = torch.zeros(max(nop, 1), dtype=torch.float32, device=self.device)
+        d.bottom_op = self._bottom_op.data_ptr() if nop > 0 else None
         self._desc = d
         h = C.c_void_p()
         N.check(N.lib().pf_mg_plan_create(C.byref(d), C.byref(h)), "pf_mg_plan_create")
@@ -158,6 +161,16 @@ class MGPCG:
     def precondition(self, r_in, z_out):
         """``z = M^-1 r``: one V-cycle, mean removed (pfflip/poisson.py:345-352)."""
         N.call("pf_mg_precondition", self._plan, N.ptr(as_tensor(r_in)), N.ptr(as_tensor(z_out)), N.stream())
+
+    def bottom_info(self):
+        """``(first_level, cluster_levels, dense)`` of the kernel that runs the
+        coarse end of the V-cycle: cluster_levels > 0 for the CTA-cluster
+        kernel, 0 for the single-CTA one; dense = 1 when the levels below the
+        cluster's slabs run as a dense operator (diagnostics; no reference
+        counterpart)."""
+        first, nd, dense = C.c_int32(0), C.c_int32(0), C.c_int32(0)
+        N.call("pf_mg_bottom_info", self._plan, C.byref(first), C.byref(nd), C.byref(dense))
+        return int(first.value), int(nd.value), int(dense.value)
 
     # ------------------------------------------------------------ solve
     def solve(self, b, p_out, *, tol=1e-4, max_iter=200, verbose=False):

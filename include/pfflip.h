@@ -299,6 +299,10 @@ typedef struct pf_mg_desc {
   void* state;
   double* partials;
   uint32_t* counters;
+  /* optional (NULL = off): pf_mg_bottom_op_floats(desc) floats for the dense
+   * operator of the V-cycle's smallest levels, rebuilt by every
+   * pf_mg_build_hierarchy (see pf_mg_bottom_info) */
+  float* bottom_op;
 } pf_mg_desc;
 
 typedef struct pf_mg_plan pf_mg_plan;
@@ -310,6 +314,22 @@ int64_t pf_mg_partials_count(void);
 int32_t pf_mg_level_count(int32_t nx, int32_t ny, int32_t nz, int32_t min_dim, int32_t* dims_out);
 int pf_mg_plan_create(const pf_mg_desc* desc, pf_mg_plan** out);
 int pf_mg_plan_destroy(pf_mg_plan* plan);
+/* Which kernel runs the coarse end of the plan's V-cycle (no reference
+ * counterpart; diagnostics).  *first_level: the finest level it covers (nlev:
+ * none); *cluster_levels: > 0 when it is the cluster kernel (one cluster of
+ * 8 CTAs; that many levels from first_level split into slabs across the CTAs),
+ * 0 for the single-CTA kernel; *dense: 1 when the levels below the slabs are
+ * applied as a dense operator (desc->bottom_op), 0 when CTA 0 sweeps them.
+ * The cluster kernel is used whenever the levels allow it; the environment
+ * variable PFFLIP_MG_BOTTOM, read at plan creation, selects "cta" (single-CTA
+ * kernel) or "cluster" (cluster kernel without the dense operator). */
+int pf_mg_bottom_info(const pf_mg_plan* plan, int32_t* first_level, int32_t* cluster_levels, int32_t* dense);
+/* Floats desc->bottom_op must hold for the plan that desc would create (0: the
+ * dense bottom does not apply to these levels).  The dense operator is the
+ * exact linear map of the V-cycle below the cluster's slabs (pre-smoothing,
+ * restriction, coarsest sweeps with mean removal, prolongation,
+ * post-smoothing), built column by column from unit right-hand sides. */
+int64_t pf_mg_bottom_op_floats(const pf_mg_desc* desc);
 /* pfflip/poisson.py:295-309 build_hierarchy: level-0 faces = (bx, by, bz),
  * per level diag = sum of 6 faces, coarse face = sum of the 2x2 fine faces in
  * plane 2I.  Also fills the 16-bit copies in mixed precision. */

@@ -236,3 +236,75 @@ def test_mixed_precision_step_matches_fp32_step(precision):
     p32 = out["fp32"][1] - out["fp32"][1].mean()
     pm = out[precision][1] - out[precision][1].mean()
     assert rel_err(pm, p32) < 1e-5
+
+
+BOTTOM_MODES = {"cta": (False, False), "cluster": (True, False), "": (True, True)}  # env -> (cluster, dense)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+@pytest.mark.parametrize("res", [(32, 32, 32), (64, 64, 64), (128, 64, 32)])
+def test_cluster_bottom_matches_single_cta_bottom(res, precision, monkeypatch):
+    """The coarse end of the V-cycle on one CTA cluster (slabs in distributed
+    shared memory; below them CTA 0's sweeps or the dense operator) against
+    the single-CTA kernel: the same iteration count within 1, all converged,
+    solutions within 1e-5 (FP32) / 1e-4 (FP16) of their maximum after
+    removing the mean."""
+    bx, by, bz, b, _ = scenes.solve_problem(res, seed=12)
+    out = {}
+    for mode, (cluster, dense) in BOTTOM_MODES.items():
+        monkeypatch.setenv("PFFLIP_MG_BOTTOM", mode)
+        g = MGPCG(res, DEV, pre=3, post=3, precision=precision)
+        first, nd, dn = g.bottom_info()
+        assert (nd > 0, dn == 1) == (cluster, dense), (mode, first, nd, dn)
+        g.build_hierarchy(dev(bx), dev(by), dev(bz))
+        x = DeviceArray.zeros(res, device=DEV)
+        it, rel = g.solve(dev(b), x, tol=1e-6, max_iter=100)
+        xv = x.numpy().astype(np.float64)
+        out[mode] = (it, rel, xv - xv.mean())
+    i1, r1, x1 = out["cta"]
+    tol = 1e-5 if precision == "fp32" else 1e-4
+    for mode in ("cluster", ""):
+        i2, r2, x2 = out[mode]
+        assert r1 < 1e-6 and r2 < 1e-6, (mode, r1, r2)
+        assert abs(i1 - i2) <= 1, (mode, i1, i2)
+        assert np.abs(x1 - x2).max() <= tol * np.abs(x1).max(), mode
+
+
+def test_cluster_bottom_precondition_matches_single_cta(monkeypatch):
+    """One V-cycle (pf_mg_precondition) with the whole 32^3 hierarchy inside
+    the cluster kernel (top level = level 0, so the mean comes from the
+    cluster's partial sums), with and without the dense operator, against the
+    single-CTA bottom."""
+    res = (32, 32, 32)
+    bx, by, bz, b, _ = scenes.solve_problem(res, seed=13)
+    z = {}
+    for mode in BOTTOM_MODES:
+        monkeypatch.setenv("PFFLIP_MG_BOTTOM", mode)
+        g = MGPCG(res, DEV, pre=2, post=2)
+        g.build_hierarchy(dev(bx), dev(by), dev(bz))
+        out = DeviceArray.zeros(res, device=DEV)
+        g.precondition(dev(b), out)
+        z[mode] = out.numpy().astype(np.float64)
+    for mode in ("cluster", ""):
+        assert abs(z[mode].mean()) < 1e-6 * np.abs(z[mode]).max()
+        assert np.abs(z["cta"] - z[mode]).max() <= 1e-5 * np.abs(z["cta"]).max(), mode
+
+
+def test_dense_bottom_operator_is_rebuilt_with_the_hierarchy(monkeypatch):
+    """The dense operator follows the coefficients: after a second
+    build_hierarchy with other faces, the dense path still agrees with the
+    single-CTA bottom."""
+    res = (64, 64, 64)
+    probs = [scenes.solve_problem(res, seed=s) for s in (21, 22)]
+    res_x = {}
+    for mode in ("cta", ""):
+        monkeypatch.setenv("PFFLIP_MG_BOTTOM", mode)
+        g = MGPCG(res, DEV, pre=2, post=2)
+        for k, (bx, by, bz, b, _) in enumerate(probs):
+            g.build_hierarchy(dev(bx), dev(by), dev(bz))
+            out = DeviceArray.zeros(res, device=DEV)
+            g.precondition(dev(b), out)
+            res_x[(mode, k)] = out.numpy().astype(np.float64)
+    for k in range(2):
+        a, c = res_x[("cta", k)], res_x[("", k)]
+        assert np.abs(a - c).max() <= 1e-5 * np.abs(a).max(), k
