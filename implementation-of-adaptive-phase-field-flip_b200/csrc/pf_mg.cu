@@ -2324,9 +2324,10 @@ int launch_sweep(pf_mg_plan* P, int lv, const T* p_in, bool zero_in, T* p_out, c
   dim3 grid((L.nz + SW_TK - 1) / SW_TK, (L.ny + SW_TJ - 1) / SW_TJ, (L.nx + TI - 1) / TI);
   if constexpr (std::is_same<T, float>::value && std::is_same<TB, float>::value) {
     TileMaps maps;
-    // large levels: 8-plane tiles (1.33 relaxations and 44 staged bytes per
-    // cell instead of 1.5 and 55), 512 threads, two CTAs per SM
-    if (P->use_tma && L.nx >= 128 && tma_maps<8, T, TB>(P, lv, p_in, b, b_scale, V, &maps)) {
+    // levels of 64+ planes: 8-plane tiles (1.33 relaxations and 44 staged
+    // bytes per cell instead of 1.5 and 55), 512 threads, two CTAs per SM (a
+    // 64^3 level is then one wave of 128 CTAs)
+    if (P->use_tma && L.nx >= 64 && tma_maps<8, T, TB>(P, lv, p_in, b, b_scale, V, &maps)) {
       const dim3 g8(grid.x, grid.y, (L.nx + 7) / 8);
       k_rb_tile_tma<8, 512><<<g8, 512, TmaDims<8>::SMEM, s>>>(maps, a);
       PF_LAUNCHED();
