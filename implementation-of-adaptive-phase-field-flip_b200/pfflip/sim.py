@@ -218,7 +218,9 @@ class Simulator:
         p4, v4 = self._pos4, self._vel4
         p4[:, :3].copy_(pos, non_blocking=True)
         v4[:, :3].copy_(vel, non_blocking=True)
-        p4.view(torch.int32)[:, 3].copy_((ptype == 1).to(torch.int32), non_blocking=True)
+        # the liquid flag is formed on the device: a host-side comparison would
+        # be a CPU pass over n values and an unpinned copy
+        p4.view(torch.int32)[:, 3].copy_((ptype.to(dev, non_blocking=True) == 1).to(torch.int32))
         v4.view(torch.int32)[:, 3] = torch.arange(n, dtype=torch.int32, device=dev)
         if self.cfg.droplets:
             self._drop_r.zero_()
