@@ -242,13 +242,14 @@ BOTTOM_MODES = {"cta": (False, False), "cluster": (True, False), "": (True, True
 
 
 @pytest.mark.parametrize("precision", ["fp32", "fp16"])
-@pytest.mark.parametrize("res", [(32, 32, 32), (64, 64, 64), (128, 64, 32)])
+@pytest.mark.parametrize("res", [(32, 32, 32), (64, 64, 64), (128, 64, 32), (64, 48, 80)])
 def test_cluster_bottom_matches_single_cta_bottom(res, precision, monkeypatch):
     """The coarse end of the V-cycle on one CTA cluster (slabs in distributed
     shared memory; below them CTA 0's sweeps or the dense operator) against
     the single-CTA kernel: the same iteration count within 1, all converged,
     solutions within 1e-5 (FP32) / 1e-4 (FP16) of their maximum after
-    removing the mean."""
+    removing the mean.  (64, 48, 80) has levels that are not powers of two
+    (division indexing) and a 480-cell dense operator."""
     bx, by, bz, b, _ = scenes.solve_problem(res, seed=12)
     out = {}
     for mode, (cluster, dense) in BOTTOM_MODES.items():
