@@ -138,40 +138,63 @@ __global__ void k_scatter(long long n, const int* __restrict__ keys, int* __rest
 
 // one warp per cell: rank the segment's original indices (distinct) so the
 // segment becomes ascending; also writes the sorted keys
+// One warp per batch of 32 consecutive cells: lane i loads the bounds of cell
+// c0 + i (one coalesced pair of loads for the batch), then the warp walks the
+// batch, writing the sorted keys of each cell and ranking its segment, with the
+// next cell's segment loaded while the current one is checked.
+__device__ __forceinline__ void fix_segment(int s, int len, int v, int c, int lane, int* __restrict__ perm,
+                                            int* __restrict__ keys_out) {
+  for (int t = s + lane; t < s + len; t += 32) keys_out[t] = c;
+  if (len <= 1) return;
+  if (len <= 32) {
+    // already ascending?  (the common case: arrivals were in order)
+    const int nxt = __shfl_down_sync(0xffffffffu, v, 1);
+    const bool ok = (lane >= len - 1) || (v < nxt);
+    if (__all_sync(0xffffffffu, ok)) return;
+    int rank = 0;
+    for (int q = 0; q < len; ++q) rank += (__shfl_sync(0xffffffffu, v, q) < v);
+    __syncwarp();
+    if (lane < len) perm[s + rank] = v;
+  } else {
+    // long segment (> 32 particles in one cell): insertion sort by one lane.
+    // Arrivals are nearly ascending, so this is close to linear in practice.
+    if (lane == 0) {
+      for (int t = s + 1; t < s + len; ++t) {
+        const int w = perm[t];
+        int u = t - 1;
+        while (u >= s && perm[u] > w) {
+          perm[u + 1] = perm[u];
+          --u;
+        }
+        perm[u + 1] = w;
+      }
+    }
+    __syncwarp();
+  }
+}
+
 __global__ void k_fix_order(int ncells, const int* __restrict__ start, int* __restrict__ perm,
                             int* __restrict__ keys_out) {
   const int lane = threadIdx.x & 31;
+  const int nbatch = (ncells + 31) >> 5;
   const int warps = (gridDim.x * blockDim.x) >> 5;
-  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < ncells; c += warps) {
-    const int s = start[c], e = start[c + 1], len = e - s;
-    if (len == 0) continue;
-    for (int t = s + lane; t < e; t += 32) keys_out[t] = c;
-    if (len == 1) continue;
-    if (len <= 32) {
-      const int v = (lane < len) ? perm[s + lane] : INT_MAX;
-      // already ascending?  (the common case: arrivals were in order)
-      const int nxt = __shfl_down_sync(0xffffffffu, v, 1);
-      const bool ok = (lane >= len - 1) || (v < nxt);
-      if (__all_sync(0xffffffffu, ok)) continue;
-      int rank = 0;
-      for (int q = 0; q < len; ++q) rank += (__shfl_sync(0xffffffffu, v, q) < v);
-      __syncwarp();
-      if (lane < len) perm[s + rank] = v;
-    } else {
-      // long segment (> 32 particles in one cell): insertion sort by one lane.
-      // Arrivals are nearly ascending, so this is close to linear in practice.
-      if (lane == 0) {
-        for (int t = s + 1; t < e; ++t) {
-          const int v = perm[t];
-          int u = t - 1;
-          while (u >= s && perm[u] > v) {
-            perm[u + 1] = perm[u];
-            --u;
-          }
-          perm[u + 1] = v;
-        }
+  for (int bt = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; bt < nbatch; bt += warps) {
+    const int c0 = bt << 5, nb = min(32, ncells - c0);
+    const int my_s = lane < nb ? start[c0 + lane] : 0;
+    const int my_e = lane < nb ? start[c0 + lane + 1] : 0;
+    int s = __shfl_sync(0xffffffffu, my_s, 0), len = __shfl_sync(0xffffffffu, my_e, 0) - s;
+    int v = (lane < len && len <= 32) ? perm[s + lane] : INT_MAX;
+    for (int q = 0; q < nb; ++q) {
+      int s2 = 0, len2 = 0, v2 = INT_MAX;
+      if (q + 1 < nb) {  // the next cell's segment, in flight while this one is checked
+        s2 = __shfl_sync(0xffffffffu, my_s, q + 1);
+        len2 = __shfl_sync(0xffffffffu, my_e, q + 1) - s2;
+        v2 = (lane < len2 && len2 <= 32) ? perm[s2 + lane] : INT_MAX;
       }
-      __syncwarp();
+      fix_segment(s, len, v, c0 + q, lane, perm, keys_out);
+      s = s2;
+      len = len2;
+      v = v2;
     }
   }
 }
@@ -230,7 +253,7 @@ int pf_sort_particles(const pf_grid* g, int64_t n, const float* pos4_in, const f
   if (n == 0) return PF_OK;
   k_scatter<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, keys_tmp, cursor, perm_out);
   PF_LAUNCHED();
-  k_fix_order<<<grid_for(nc * 32, 256, kNumSMs * 16), 256, 0, s>>>((int)nc, cell_start, perm_out, keys_out);
+  k_fix_order<<<grid_for(nc, 256, 1 << 20), 256, 0, s>>>((int)nc, cell_start, perm_out, keys_out);
   PF_LAUNCHED();
   k_gather<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, perm_out, reinterpret_cast<const float4*>(pos4_in),
                                                           reinterpret_cast<const float4*>(vel4_in),
@@ -347,7 +370,7 @@ extern "C" int pf_sort_particles_static(const pf_grid* g, int64_t n, const float
   if (n == 0) return PF_OK;
   k_scatter_rank<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, key_rank, cell_start, perm_out);
   PF_LAUNCHED();
-  k_fix_order<<<grid_for(nc * 32, 256, kNumSMs * 16), 256, 0, s>>>((int)nc, cell_start, perm_out, keys_out);
+  k_fix_order<<<grid_for(nc, 256, 1 << 20), 256, 0, s>>>((int)nc, cell_start, perm_out, keys_out);
   PF_LAUNCHED();
   k_gather<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, perm_out, reinterpret_cast<const float4*>(pos4_in),
                                                           reinterpret_cast<const float4*>(vel4_in),
