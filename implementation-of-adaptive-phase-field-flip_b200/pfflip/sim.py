@@ -107,6 +107,7 @@ class ParticleField:
 
     def assign(self, a):
         s, k = self._sim, self._kind
+        s._fresh_sort = False
         ids = s._ids().long()
         t = torch.as_tensor(np.ascontiguousarray(np.asarray(a))).to(s.dev)
         if k in ("pos", "vel"):
@@ -165,6 +166,9 @@ class Simulator:
         )
 
         self.n_particles = 0
+        # True only between set_particles (which sorts) and the next stage: the
+        # step's own sort would then repeat it on the same particles
+        self._fresh_sort = False
         self._pos4 = self._vel4 = None
         self.droplet_stats = {"emitted": 0, "bubbles": 0, "merged": 0, "spray": 0}
 
@@ -225,6 +229,7 @@ class Simulator:
         if self.cfg.droplets:
             self._drop_r.zero_()
         self._sort()
+        self._fresh_sort = True
 
     def read_particles(self, pos_out=None, vel_out=None):
         """Positions and velocities in the original order, copied into the given
@@ -366,7 +371,10 @@ class Simulator:
         cfg = self.cfg
         if mark:
             mark("sort")
-        self._sort()
+        if self._fresh_sort:  # set_particles sorted these very particles
+            self._fresh_sort = False
+        else:
+            self._sort()
         if mark:
             mark("p2g")
         N.call("pf_p2g", C.byref(self._g), self.n_particles, self._pos4.data_ptr(), self._vel4.data_ptr(),
@@ -430,6 +438,7 @@ class Simulator:
         return lo, hi
 
     def _g2p_advect(self, dt, do_g2p, do_advect):
+        self._fresh_sort = False
         lo, hi = self._bounds()
         cfg = self.cfg
         if self._g2p_ws is None:
@@ -452,6 +461,7 @@ class Simulator:
 
     def _droplets(self, dt: float):
         """Escaped particles -> droplets, droplet dynamics (pfflip/sim.py:343-392)."""
+        self._fresh_sort = False
         cfg = self.cfg
         if not cfg.droplets or self.n_particles == 0:
             return
