@@ -220,11 +220,34 @@ class Simulator:
             self._alloc_particles(n)
         self.n_particles = n
         p4, v4 = self._pos4, self._vel4
-        p4[:, :3].copy_(pos, non_blocking=True)
-        v4[:, :3].copy_(vel, non_blocking=True)
+        main = torch.cuda.current_stream(dev)
+        if pos.device.type == "cpu" and vel.device.type == "cpu" and ptype.device.type == "cpu":
+            # host arrays: the three uploads run on a copy stream, each one
+            # overlapping the packing of the previous array on this stream
+            cs = self._copy_stream()
+            cs.wait_stream(main)
+            staged = []
+            with torch.cuda.stream(cs):
+                for a in (pos, vel, ptype):
+                    d = a.to(dev, non_blocking=True)
+                    staged.append((d, cs.record_event()))
+            for d, _ in staged:
+                d.record_stream(main)
+            (dpos, ep), (dvel, ev), (dpt, et) = staged
+        else:
+            dpos, dvel, dpt = pos.to(dev), vel.to(dev), ptype.to(dev)
+            ep = ev = et = None
+        if ep is not None:
+            main.wait_event(ep)
+        p4[:, :3].copy_(dpos)
+        if ev is not None:
+            main.wait_event(ev)
+        v4[:, :3].copy_(dvel)
+        if et is not None:
+            main.wait_event(et)
         # the liquid flag is formed on the device: a host-side comparison would
         # be a CPU pass over n values and an unpinned copy
-        p4.view(torch.int32)[:, 3].copy_((ptype.to(dev, non_blocking=True) == 1).to(torch.int32))
+        p4.view(torch.int32)[:, 3].copy_((dpt == 1).to(torch.int32))
         v4.view(torch.int32)[:, 3] = torch.arange(n, dtype=torch.int32, device=dev)
         if self.cfg.droplets:
             self._drop_r.zero_()
@@ -233,18 +256,39 @@ class Simulator:
 
     def read_particles(self, pos_out=None, vel_out=None):
         """Positions and velocities in the original order, copied into the given
-        (pinned) host tensors when provided; returns (pos, vel)."""
+        (pinned) host tensors when provided; returns (pos, vel).  With host
+        tensors given, the copy of the positions runs on a copy stream while
+        the velocities are put back in order; the caller's stream waits for
+        both copies."""
         ids = self._ids().long()
+        main = torch.cuda.current_stream(self.dev)
         out = []
+        copied = False
         for src, dst in ((self._pos4, pos_out), (self._vel4, vel_out)):
             tmp = torch.empty((self.n_particles, 3), dtype=torch.float32, device=self.dev)
             tmp[ids] = src[:, :3]
             if dst is None:
                 out.append(tmp.cpu())
-            else:
-                dst.copy_(tmp, non_blocking=True)
+            elif dst.device.type == "cpu":
+                cs = self._copy_stream()
+                cs.wait_stream(main)
+                with torch.cuda.stream(cs):
+                    dst.copy_(tmp, non_blocking=True)
+                tmp.record_stream(cs)
+                copied = True
                 out.append(dst)
+            else:
+                dst.copy_(tmp)
+                out.append(dst)
+        if copied:
+            main.wait_stream(self._copy_stream())
         return tuple(out)
+
+    def _copy_stream(self):
+        """The side stream of host<->device particle copies."""
+        if getattr(self, "_cstream", None) is None:
+            self._cstream = torch.cuda.Stream(device=self.dev)
+        return self._cstream
 
     def _alloc_particles(self, n):
         dev = self.dev
