@@ -169,6 +169,7 @@ class Simulator:
         # True only between set_particles (which sorts) and the next stage: the
         # step's own sort would then repeat it on the same particles
         self._fresh_sort = False
+        self._pending_d2h = []  # (host lo, host hi, event) of read_particles' chunked downloads
         self._pos4 = self._vel4 = None
         self.droplet_stats = {"emitted": 0, "bubbles": 0, "merged": 0, "spray": 0}
 
@@ -222,18 +223,20 @@ class Simulator:
         p4, v4 = self._pos4, self._vel4
         main = torch.cuda.current_stream(dev)
         if pos.device.type == "cpu" and vel.device.type == "cpu" and ptype.device.type == "cpu":
-            # host arrays: the three uploads run on a copy stream, each one
-            # overlapping the packing of the previous array on this stream
-            cs = self._copy_stream()
-            cs.wait_stream(main)
-            staged = []
-            with torch.cuda.stream(cs):
-                for a in (pos, vel, ptype):
-                    d = a.to(dev, non_blocking=True)
-                    staged.append((d, cs.record_event()))
-            for d, _ in staged:
+            # host arrays: the uploads run on the upload stream, each one
+            # overlapping the packing of the previous array on this stream.
+            # A host range that read_particles is still filling is uploaded
+            # chunk by chunk behind the download of that range (see _upload)
+            up = self._copy_streams()[1]
+            pending, self._pending_d2h = self._pending_d2h, []
+            staged = {}
+            with torch.cuda.stream(up):
+                for name, a in (("t", ptype), ("p", pos), ("v", vel)):  # the types first: nothing writes them
+                    d = self._upload(a, pending, up)
+                    staged[name] = (d, up.record_event())
+            for d, _ in staged.values():
                 d.record_stream(main)
-            (dpos, ep), (dvel, ev), (dpt, et) = staged
+            (dpos, ep), (dvel, ev), (dpt, et) = staged["p"], staged["v"], staged["t"]
         else:
             dpos, dvel, dpt = pos.to(dev), vel.to(dev), ptype.to(dev)
             ep = ev = et = None
@@ -256,39 +259,75 @@ class Simulator:
 
     def read_particles(self, pos_out=None, vel_out=None):
         """Positions and velocities in the original order, copied into the given
-        (pinned) host tensors when provided; returns (pos, vel).  With host
-        tensors given, the copy of the positions runs on a copy stream while
-        the velocities are put back in order; the caller's stream waits for
-        both copies."""
+        (pinned) host tensors when provided; returns (pos, vel).
+
+        With contiguous host tensors given, each copy runs on the download
+        stream in chunks of _CHUNK bytes, the positions' copy overlapping the
+        reordering of the velocities; the caller's stream waits for both.  The
+        chunks' events stay recorded, so that a set_particles from these same
+        host buffers uploads each chunk as soon as its download has landed."""
         ids = self._ids().long()
         main = torch.cuda.current_stream(self.dev)
         out = []
         copied = False
+        pending = []
         for src, dst in ((self._pos4, pos_out), (self._vel4, vel_out)):
             tmp = torch.empty((self.n_particles, 3), dtype=torch.float32, device=self.dev)
             tmp[ids] = src[:, :3]
             if dst is None:
                 out.append(tmp.cpu())
-            elif dst.device.type == "cpu":
-                cs = self._copy_stream()
-                cs.wait_stream(main)
-                with torch.cuda.stream(cs):
-                    dst.copy_(tmp, non_blocking=True)
-                tmp.record_stream(cs)
+            elif dst.device.type == "cpu" and dst.is_contiguous():
+                down = self._copy_streams()[0]
+                down.wait_stream(main)
+                fd, ft = dst.view(-1), tmp.view(-1)
+                step = self._CHUNK // 4
+                with torch.cuda.stream(down):
+                    for off in range(0, fd.numel(), step):
+                        m = min(step, fd.numel() - off)
+                        fd[off:off + m].copy_(ft[off:off + m], non_blocking=True)
+                        lo = dst.data_ptr() + 4 * off
+                        pending.append((lo, lo + 4 * m, down.record_event()))
+                tmp.record_stream(down)
                 copied = True
                 out.append(dst)
             else:
                 dst.copy_(tmp)
                 out.append(dst)
         if copied:
-            main.wait_stream(self._copy_stream())
+            main.wait_stream(self._copy_streams()[0])
+        self._pending_d2h = pending
         return tuple(out)
 
-    def _copy_stream(self):
-        """The side stream of host<->device particle copies."""
-        if getattr(self, "_cstream", None) is None:
-            self._cstream = torch.cuda.Stream(device=self.dev)
-        return self._cstream
+    _CHUNK = 1 << 25  # bytes per chunk of a host<->device particle copy
+
+    def _copy_streams(self):
+        """(download, upload) side streams of the host<->device particle copies."""
+        if getattr(self, "_cstreams", None) is None:
+            self._cstreams = (torch.cuda.Stream(device=self.dev), torch.cuda.Stream(device=self.dev))
+        return self._cstreams
+
+    def _upload(self, a, pending, stream):
+        """Device copy of host array a, enqueued on `stream` (the current
+        stream), chunk by chunk; a chunk whose host bytes overlap a pending
+        download waits for that download's event."""
+        d = torch.empty(a.shape, dtype=a.dtype, device=self.dev)
+        if not pending or not a.is_contiguous():
+            for _, _, ev in pending:
+                stream.wait_event(ev)
+            d.copy_(a, non_blocking=True)
+            return d
+        fa, fd = a.view(-1), d.view(-1)
+        es = a.element_size()
+        step = self._CHUNK // es
+        for off in range(0, fa.numel(), step):
+            m = min(step, fa.numel() - off)
+            lo = a.data_ptr() + es * off
+            hi = lo + es * m
+            for b0, b1, ev in pending:
+                if b0 < hi and lo < b1:
+                    stream.wait_event(ev)
+            fd[off:off + m].copy_(fa[off:off + m], non_blocking=True)
+        return d
 
     def _alloc_particles(self, n):
         dev = self.dev

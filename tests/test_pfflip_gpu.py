@@ -239,3 +239,60 @@ def test_save_frame_writes_the_reference_format(tmp_path):
     assert np.array_equal(f["ptype"], pt[::3].astype(np.int8))
     io.save_frame(sim, str(tmp_path / "f2.npz"), particles=False)
     assert set(io.load_frame(str(tmp_path / "f2.npz"))) == {"t", "step", "dx", "phi"}
+
+
+def test_host_round_trip_with_overlapped_copies_is_exact(monkeypatch):
+    """set_particles from the very host buffers read_particles is still filling
+    (chunked downloads; each upload chunk waits for the download of its host
+    bytes) delivers every chunk's new contents.  Between upload and download a
+    deterministic device update changes every value (the step itself sums with
+    atomics, so it is not bitwise repeatable); an upload that raced its
+    download would bring back stale values.  Small chunks, so that each array
+    spans many of them."""
+    import torch
+
+    monkeypatch.setattr(Simulator, "_CHUNK", 1 << 16)
+    cfg = Config(res=(32,) * 3, dx=1 / 32, ppc=8, droplets=False)
+    pos, vel, pt = scenes.dam_break(cfg)
+    exp_p, exp_v = pos.copy(), vel.copy()
+    for _ in range(4):
+        exp_p = exp_p + np.float32(1e-3)
+        exp_v = exp_v * np.float32(1.5)
+    for sync in (False, True):
+        sim = Simulator(cfg)
+        hp = torch.from_numpy(pos.copy()).pin_memory()
+        hv = torch.from_numpy(vel.copy()).pin_memory()
+        ht = torch.from_numpy(pt.astype(np.int32)).pin_memory()
+        for _ in range(4):
+            sim.set_particles(hp, hv, ht)
+            sim._pos4[:, :3] += 1e-3
+            sim._vel4[:, :3] *= 1.5
+            if not sync:
+                torch.cuda._sleep(20_000_000)  # ~10 ms: the next uploads are queued before these downloads run
+            sim.read_particles(hp, hv)
+            if sync:
+                torch.cuda.synchronize()
+        torch.cuda.synchronize()
+        assert np.array_equal(hp.numpy(), exp_p), sync
+        assert np.array_equal(hv.numpy(), exp_v), sync
+
+
+def test_host_round_trip_steps_read_back_the_device_state():
+    """Whole steps through pinned host buffers: after the last read the host
+    arrays are exactly the simulator's particles in the caller's order."""
+    import torch
+
+    cfg = Config(res=(32,) * 3, dx=1 / 32, ppc=8, droplets=False)
+    pos, vel, pt = scenes.dam_break(cfg)
+    dt = 0.5 * cfg.dx / math.sqrt(2 * 9.81 * 0.6)
+    sim = Simulator(cfg)
+    hp = torch.from_numpy(pos.copy()).pin_memory()
+    hv = torch.from_numpy(vel.copy()).pin_memory()
+    ht = torch.from_numpy(pt.astype(np.int32)).pin_memory()
+    for _ in range(3):
+        sim.set_particles(hp, hv, ht)
+        sim.step(dt)
+        sim.read_particles(hp, hv)
+    torch.cuda.synchronize()
+    assert np.array_equal(hp.numpy(), sim.px.numpy()) and np.array_equal(hv.numpy(), sim.pv.numpy())
+    assert np.abs(hp.numpy() - pos).max() > 0
