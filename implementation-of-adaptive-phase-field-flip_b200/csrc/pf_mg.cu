@@ -2674,6 +2674,10 @@ int solve_impl(pf_mg_plan* P, const float* b, float* x, float tol, int max_iter,
     set_error(PF_ERR_NONFINITE, "non-finite residual in the CG iteration %d", h->it);
     return PF_ERR_NONFINITE;
   }
+  if (h->status == ST_TMA_TIMEOUT) {
+    set_error(PF_ERR_CUDA, "a TMA staging wait timed out in the CG iteration %d; the solve was stopped", h->it);
+    return PF_ERR_CUDA;
+  }
   if (h->status == ST_RUNNING) {
     set_error(PF_ERR_NOT_CONVERGED, "tolerance %g not reached in %d iterations (rel %g)", (double)tol, h->it, h->rel);
     return PF_ERR_NOT_CONVERGED;
