@@ -12,7 +12,6 @@
 // for power-of-two dx, within an ulp otherwise.
 // Particles are in cell order, so neighbouring threads gather neighbouring
 // taps from L1/L2.
-#include "pf_f32x2.cuh"
 #include "pf_faces.cuh"
 
 namespace pf {
@@ -188,20 +187,22 @@ __global__ void __launch_bounds__(256) k_g2p_advect(G2PArgs a) {
 }
 
 // ---------------------------------------------------------------- paired taps
-// The same particle pass reading the face fields through k-paired copies:
-// uu[c][f] = (u[f], u[f+1], u*[f], u*[f+1]) and ul[c][f] = (ul[f], ul[f+1])
-// along k (f+1 -> f on the last k plane).  A trilinear sample then needs four
-// row loads (one per (i, j) tap pair) instead of eight gathers, and G2P reads u
-// and u* with one 16-byte load per row.  Where the frame clamps the k taps to
-// one index (lo == hi) the upper tap takes the lower value, so every tap value
-// and every sum is the one the unpaired kernel forms.
+// The same particle pass reading the face fields through quads: for every face
+// f = (i, j, k) of a face grid, q[f] = (v[j][k], v[j][k+1], v[j+1][k],
+// v[j+1][k+1]) of the same i-plane, with j+1 -> j and k+1 -> k on the last
+// plane of the grid.  A trilinear sample is then two 16-byte loads (the lower
+// and the upper i-plane) instead of eight gathers.  Where the frame clamps
+// the j or k taps to one index (lo == hi) the upper taps take the lower
+// values, so every tap value is the one the unpaired kernel reads.  u, u* and
+// the extrapolated field ul each get their quads.
 struct FacePack {
   FaceSpace s;
   const float* u[3];
   const float* us[3];
   const float* ul[3];
-  float4* uu[3];
-  float2* ul2[3];
+  float4* qu[3];
+  float4* qs[3];
+  float4* ql[3];
 };
 
 struct G2PPackedArgs {
@@ -211,8 +212,9 @@ struct G2PPackedArgs {
   float lo[3], hi[3];
   float4* pos;
   float4* vel;
-  const float4* uu[3];
-  const float2* ul[3];
+  const float4* qu[3];
+  const float4* qs[3];
+  const float4* ql[3];
   const int* solid;
   int do_g2p, do_advect;
 };
@@ -222,83 +224,66 @@ __global__ void __launch_bounds__(C3_NT) k_pack_faces(FacePack fp) {
   int i, j, k;
   const int ax = locate(fp.s, &f, &i, &j, &k);
   if (ax < 0 || ax > 2) return;
-  const int n2 = fp.s.nz + (ax == 2);
-  const long long fn = (k < n2 - 1) ? f + 1 : f;
+  const int n1 = fp.s.ny + (ax == 1), n2 = fp.s.nz + (ax == 2);
+  const long long dk = (k < n2 - 1) ? 1 : 0, dj = (j < n1 - 1) ? n2 : 0;
   const float* u = fp.u[ax];
-  const float* us = fp.us[ax];
-  fp.uu[ax][f] = make_float4(u[f], u[fn], us ? us[f] : 0.f, us ? us[fn] : 0.f);
-  if (fp.ul2[ax]) fp.ul2[ax][f] = make_float2(fp.ul[ax][f], fp.ul[ax][fn]);
+  fp.qu[ax][f] = make_float4(u[f], u[f + dk], u[f + dj], u[f + dj + dk]);
+  if (const float* us = fp.us[ax]) fp.qs[ax][f] = make_float4(us[f], us[f + dk], us[f + dj], us[f + dj + dk]);
+  if (const float* ul = fp.ul[ax]) fp.ql[ax][f] = make_float4(ul[f], ul[f + dk], ul[f + dj], ul[f + dj + dk]);
 }
 
-// (di, dj) row offsets and k-tap selection of face grid c for a frame
+// the two i-planes of face grid c for a frame, and the (j, k) weights
 struct Rows {
-  int row[4];
-  float wij[4];
-  float wk0, wk1;
-  bool clampk;
+  int row[2];
+  float wi[2];
+  float wj0, wj1, wk0, wk1;
+  bool cj, ck;  // j / k taps clamped to one index
 };
 
 __device__ __forceinline__ void rows_of(const Frame& fr, int c, int ny, int nz, Rows& r) {
   const int vi = c == 0 ? 0 : 1, vj = c == 1 ? 0 : 1, vk = c == 2 ? 0 : 1;
   const int n1 = ny + (c == 1), n2 = nz + (c == 2);
   const float tx = fr.t[0][vi], ty = fr.t[1][vj], tz = fr.t[2][vk];
-  const int I[2] = {fr.lo[0][vi], fr.hi[0][vi]}, J[2] = {fr.lo[1][vj], fr.hi[1][vj]};
-  const float wi[2] = {1.f - tx, tx}, wj[2] = {1.f - ty, ty};
-#pragma unroll
-  for (int di = 0; di < 2; ++di)
-#pragma unroll
-    for (int dj = 0; dj < 2; ++dj) {
-      r.row[di * 2 + dj] = (I[di] * n1 + J[dj]) * n2 + fr.lo[2][vk];
-      r.wij[di * 2 + dj] = wi[di] * wj[dj];
-    }
+  const int jk = fr.lo[1][vj] * n2 + fr.lo[2][vk];
+  r.row[0] = fr.lo[0][vi] * n1 * n2 + jk;
+  r.row[1] = fr.hi[0][vi] * n1 * n2 + jk;
+  r.wi[0] = 1.f - tx;
+  r.wi[1] = tx;
+  r.wj0 = 1.f - ty;
+  r.wj1 = ty;
   r.wk0 = 1.f - tz;
   r.wk1 = tz;
-  r.clampk = fr.lo[2][vk] == fr.hi[2][vk];
+  r.cj = fr.lo[1][vj] == fr.hi[1][vj];
+  r.ck = fr.lo[2][vk] == fr.hi[2][vk];
 }
 
-// The samplers below run on packed f32x2 pairs: each row load gives the
-// (lower, upper) k taps as one pair, weighted by (w_ij w_k0, w_ij w_k1), and
-// the two halves are summed at the end.  Tap values and weights are the
-// unpaired kernel's; only the order of the final sum differs.
+// the four taps of a quad after the frame's clamps: (j, k), (j, k+1), (j+1, k), (j+1, k+1)
+__device__ __forceinline__ float4 taps(float4 v, const Rows& r) {
+  const float b = r.ck ? v.x : v.y;
+  const float d = r.ck ? v.z : v.w;
+  return r.cj ? make_float4(v.x, b, v.x, b) : make_float4(v.x, b, v.z, d);
+}
+
+__device__ __forceinline__ float bilerp(float4 t, const Rows& r) {
+  return r.wj0 * (r.wk0 * t.x + r.wk1 * t.y) + r.wj1 * (r.wk0 * t.z + r.wk1 * t.w);
+}
 
 // G2P sample of component c: delta = I(u - u*) tap by tap, pic = I(u)
-__device__ __forceinline__ void sample_g2p_packed(const float4* __restrict__ uu, const Rows& r, float& delta,
-                                                  float& pic) {
-  const f2 wk = f2_make(r.wk0, r.wk1), neg1 = f2_bcast(-1.f);
-  f2 ad = f2_bcast(0.f), ap = ad;
+__device__ __forceinline__ void sample_g2p_packed(const float4* __restrict__ qu, const float4* __restrict__ qs,
+                                                  const Rows& r, float& delta, float& pic) {
+  float ad = 0.f, ap = 0.f;
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const float4 v = __ldg(uu + r.row[q]);
-    const float u1 = r.clampk ? v.x : v.y, s1 = r.clampk ? v.z : v.w;
-    const f2 w = f2_mul(f2_bcast(r.wij[q]), wk);
-    const f2 u2 = f2_make(v.x, u1);
-    ad = f2_fma(w, f2_fma(f2_make(v.z, s1), neg1, u2), ad);
-    ap = f2_fma(w, u2, ap);
+  for (int q = 0; q < 2; ++q) {
+    const float4 u = taps(__ldg(qu + r.row[q]), r), w = taps(__ldg(qs + r.row[q]), r);
+    ad += r.wi[q] * bilerp(make_float4(u.x - w.x, u.y - w.y, u.z - w.z, u.w - w.w), r);
+    ap += r.wi[q] * bilerp(u, r);
   }
-  delta = f2_x(ad) + f2_y(ad);
-  pic = f2_x(ap) + f2_y(ap);
+  delta = ad;
+  pic = ap;
 }
 
-__device__ __forceinline__ float sample_pair2(const float2* __restrict__ f, const Rows& r) {
-  const f2 wk = f2_make(r.wk0, r.wk1);
-  f2 acc = f2_bcast(0.f);
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const float2 v = __ldg(f + r.row[q]);
-    acc = f2_fma(f2_mul(f2_bcast(r.wij[q]), wk), f2_make(v.x, r.clampk ? v.x : v.y), acc);
-  }
-  return f2_x(acc) + f2_y(acc);
-}
-
-__device__ __forceinline__ float sample_pair4(const float4* __restrict__ f, const Rows& r) {
-  const f2 wk = f2_make(r.wk0, r.wk1);
-  f2 acc = f2_bcast(0.f);
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const float4 v = __ldg(f + r.row[q]);
-    acc = f2_fma(f2_mul(f2_bcast(r.wij[q]), wk), f2_make(v.x, r.clampk ? v.x : v.y), acc);
-  }
-  return f2_x(acc) + f2_y(acc);
+__device__ __forceinline__ float sample_quad(const float4* __restrict__ q, const Rows& r) {
+  return r.wi[0] * bilerp(taps(__ldg(q + r.row[0]), r), r) + r.wi[1] * bilerp(taps(__ldg(q + r.row[1]), r), r);
 }
 
 // RK3 sample: liquid particles read the extrapolated field, air the raw one
@@ -308,11 +293,11 @@ __device__ __forceinline__ void sample_vel_packed(const G2PPackedArgs& a, bool l
   for (int c = 0; c < 3; ++c) {
     Rows r;
     rows_of(fr, c, a.ny, a.nz, r);
-    out[c] = liquid ? sample_pair2(a.ul[c], r) : sample_pair4(a.uu[c], r);
+    out[c] = sample_quad(liquid ? a.ql[c] : a.qu[c], r);
   }
 }
 
-__global__ void __launch_bounds__(256, 4) k_g2p_advect_packed(G2PPackedArgs a) {
+__global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(G2PPackedArgs a) {
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
     float4 P = a.pos[p];
     float4 V = a.vel[p];
@@ -331,7 +316,7 @@ __global__ void __launch_bounds__(256, 4) k_g2p_advect_packed(G2PPackedArgs a) {
         Rows r;
         rows_of(fx, c, a.ny, a.nz, r);
         float delta, pic;
-        sample_g2p_packed(a.uu[c], r, delta, pic);
+        sample_g2p_packed(a.qu[c], a.qs[c], r, delta, pic);
         v[c] = alpha * (v[c] + delta) + (1.f - alpha) * pic;
       }
     }
@@ -420,17 +405,15 @@ namespace {
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 // workspace layout: per axis the float4 (u, u*) pairs, then the float2 ul pairs
-size_t packed_bytes(const pf_grid* g, size_t offs[6]) {
+// workspace layout: per axis the quads of u, of u* and of the extrapolated field
+size_t packed_bytes(const pf_grid* g, size_t offs[9]) {
   const FaceSpace sp = make_space(g->nx, g->ny, g->nz);
   size_t off = 0;
-  for (int c = 0; c < 3; ++c) {
-    offs[c] = off;
-    off += align256((size_t)sp.nf[c] * sizeof(float4));
-  }
-  for (int c = 0; c < 3; ++c) {
-    offs[3 + c] = off;
-    off += align256((size_t)sp.nf[c] * sizeof(float2));
-  }
+  for (int f = 0; f < 3; ++f)
+    for (int c = 0; c < 3; ++c) {
+      offs[3 * f + c] = off;
+      off += align256((size_t)sp.nf[c] * sizeof(float4));
+    }
   return off;
 }
 
@@ -438,7 +421,7 @@ size_t packed_bytes(const pf_grid* g, size_t offs[6]) {
 
 extern "C" size_t pf_g2p_workspace_bytes(const pf_grid* g) {
   if (!g || g->nx <= 0 || g->ny <= 0 || g->nz <= 0) return 0;
-  size_t offs[6];
+  size_t offs[9];
   return packed_bytes(g, offs);
 }
 
@@ -454,7 +437,7 @@ extern "C" int pf_g2p_advect_packed(const pf_grid* g, int64_t n, float* pos4, fl
   PF_REQUIRE(!do_g2p || (vstar_x && vstar_y && vstar_z), "u* fields required for G2P");
   PF_REQUIRE(!do_advect || (vliq_x && vliq_y && vliq_z && lo && hi), "extrapolated fields and bounds required");
   PF_REQUIRE(aligned16(pos4) && aligned16(vel4), "particle streams must be 16-byte aligned");
-  size_t offs[6];
+  size_t offs[9];
   PF_REQUIRE(workspace && workspace_bytes >= packed_bytes(g, offs), "workspace too small");
   PF_REQUIRE((reinterpret_cast<uintptr_t>(workspace) & 255) == 0, "workspace must be 256-byte aligned");
   PF_REQUIRE((long long)g->nx * g->ny * (g->nz + 1) < (1LL << 31) &&
@@ -474,10 +457,12 @@ extern "C" int pf_g2p_advect_packed(const pf_grid* g, int64_t n, float* pos4, fl
     fp.u[c] = u[c];
     fp.us[c] = do_g2p ? us[c] : nullptr;
     fp.ul[c] = do_advect ? ul[c] : nullptr;
-    fp.uu[c] = reinterpret_cast<float4*>(ws + offs[c]);
-    fp.ul2[c] = do_advect ? reinterpret_cast<float2*>(ws + offs[3 + c]) : nullptr;
-    a.uu[c] = fp.uu[c];
-    a.ul[c] = fp.ul2[c];
+    fp.qu[c] = reinterpret_cast<float4*>(ws + offs[c]);
+    fp.qs[c] = do_g2p ? reinterpret_cast<float4*>(ws + offs[3 + c]) : nullptr;
+    fp.ql[c] = do_advect ? reinterpret_cast<float4*>(ws + offs[6 + c]) : nullptr;
+    a.qu[c] = fp.qu[c];
+    a.qs[c] = fp.qs[c];
+    a.ql[c] = fp.ql[c];
   }
   k_pack_faces<<<grid_faces(g->nx, g->ny, g->nz, false), C3_NT, 0, s>>>(fp);
   PF_LAUNCHED();
