@@ -361,7 +361,7 @@ struct ExSweepArgs {
   float* B[3];
 };
 
-__global__ void __launch_bounds__(C3_NT) k_adj_ex_sweep(ExSweepArgs a) {
+__global__ void __launch_bounds__(C3_NT) k_adj_ex_sweep(const __grid_constant__ ExSweepArgs a) {
   long long f;
   int i, j, k;
   const int ax = locate(a.S, &f, &i, &j, &k);
@@ -578,7 +578,7 @@ __device__ __forceinline__ void p2g_adjoint_grid(const AdjP2GArgs& a, int c, con
   }
 }
 
-__global__ void __launch_bounds__(128) k_adj_p2g(AdjP2GArgs a) {
+__global__ void __launch_bounds__(128) k_adj_p2g(const __grid_constant__ AdjP2GArgs a) {
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
     const float4 P = a.pos[p], V = a.vel[p];
     const int flags = __float_as_int(P.w);

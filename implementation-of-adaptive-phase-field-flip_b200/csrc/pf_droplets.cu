@@ -110,7 +110,7 @@ struct ClassifyArgs {
 };
 
 // pfflip/droplets.py:67-106 classify_escaped
-__global__ void __launch_bounds__(256) k_droplet_classify(ClassifyArgs a) {
+__global__ void __launch_bounds__(256) k_droplet_classify(const __grid_constant__ ClassifyArgs a) {
   int emitted = 0, bubbles = 0, merged = 0;
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
     float4 P = a.pos[p];
@@ -188,7 +188,7 @@ struct SprayArgs {
 };
 
 // pfflip/droplets.py:112-150 emit_spray_in_shear
-__global__ void __launch_bounds__(256) k_spray_emit(SprayArgs a) {
+__global__ void __launch_bounds__(256) k_spray_emit(const __grid_constant__ SprayArgs a) {
   int spray = 0;
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
     float4 P = a.pos[p];

@@ -126,7 +126,7 @@ __device__ __forceinline__ void push_out_of_solids(const int* __restrict__ solid
   }
 }
 
-__global__ void __launch_bounds__(256) k_g2p_advect(G2PArgs a) {
+__global__ void __launch_bounds__(256) k_g2p_advect(const __grid_constant__ G2PArgs a) {
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
     float4 P = a.pos[p];
     float4 V = a.vel[p];
@@ -297,7 +297,7 @@ __device__ __forceinline__ void sample_vel_packed(const G2PPackedArgs& a, bool l
   }
 }
 
-__global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(G2PPackedArgs a) {
+__global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(const __grid_constant__ G2PPackedArgs a) {
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
     float4 P = a.pos[p];
     float4 V = a.vel[p];

@@ -77,7 +77,7 @@ struct ForceArgs {
 };
 
 // vel_star = vel; vel += g*dt; walls/obstacles zeroed (pfflip/sim.py:176-177, :270-285)
-__global__ void __launch_bounds__(C3_NT) k_save_force(ForceArgs a) {
+__global__ void __launch_bounds__(C3_NT) k_save_force(const __grid_constant__ ForceArgs a) {
   const FaceSpace& S = a.s;
   {
     long long f;
@@ -129,7 +129,7 @@ struct ProjArgs {
 };
 
 // pfflip/kernels.py:366-387
-__global__ void __launch_bounds__(C3_NT) k_project(ProjArgs a) {
+__global__ void __launch_bounds__(C3_NT) k_project(const __grid_constant__ ProjArgs a) {
   const FaceSpace& S = a.s;
   {
     long long f;

@@ -1185,7 +1185,7 @@ __device__ void bt_local_vcycle(const BottomLevel* Ls, float* base, int l0, int 
 }
 
 template <class T, class TB, class AccT>
-__global__ void __launch_bounds__(BT_NT) k_bottom(BottomArgs<T, TB> a) {
+__global__ void __launch_bounds__(BT_NT) k_bottom(const __grid_constant__ BottomArgs<T, TB> a) {
   if (is_done(a.st)) return;
   extern __shared__ __align__(16) unsigned char btsm[];
   __shared__ double sred[40];
@@ -1793,7 +1793,7 @@ template <class T> struct DenseBuildArgs {
 };
 
 template <class T, class AccT>
-__global__ void __launch_bounds__(DB_NT) k_bottom_dense_build(DenseBuildArgs<T> a) {
+__global__ void __launch_bounds__(DB_NT) k_bottom_dense_build(const __grid_constant__ DenseBuildArgs<T> a) {
   extern __shared__ __align__(16) unsigned char dbsm[];
   __shared__ double sred[40];
   __shared__ double s_mean;

@@ -229,7 +229,7 @@ __device__ __forceinline__ void p2g_grid(const P2GArgs& a, float* acc, int i, in
   box.flush(acc + a1 * PG_BOX, acc + a2 * PG_BOX, li, lj, lane);
 }
 
-__global__ void __launch_bounds__(PG_NT) k_p2g(P2GArgs a) {
+__global__ void __launch_bounds__(PG_NT) k_p2g(const __grid_constant__ P2GArgs a) {
   extern __shared__ __align__(16) float acc[];  // [PG_NACC][PG_BOX]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int k0 = blockIdx.x * PG_TK, j0 = blockIdx.y * PG_TJ, i0 = blockIdx.z * PG_TI;
