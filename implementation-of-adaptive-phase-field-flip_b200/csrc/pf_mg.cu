@@ -2208,8 +2208,9 @@ template <class T> LV<T> view(pf_mg_plan* P, int lv) {
   return LV<T>{(T*)L.bx_lp, (T*)L.by_lp, (T*)L.bz_lp, (T*)L.p_lp, (T*)L.p_lp_alt, (T*)L.b_lp};
 }
 
-// one thread per element: every load of a thread is independent of the others
-int red_grid(long long n) { return grid_for(n, RED_NT, (int)(pf::kPartials / 2)); }
+// about 8 CTAs per SM: each thread runs several elements of a grid-stride
+// loop, so several loads are in flight per thread
+int red_grid(long long n) { return grid_for(n, RED_NT, kNumSMs * 8); }
 // 4-wide grid-stride kernels: about 8 CTAs per SM
 int vec_grid(long long n) { return grid_for((n + 3) / 4, RED_NT, kNumSMs * 8); }
 int ew_grid(long long n) { return grid_for(n, 256, 1 << 20); }
