@@ -38,6 +38,33 @@ __host__ inline dim3 grid_faces(int nx, int ny, int nz, bool with_cells) {
   return dim3((unsigned)((nz + 1 + C3_TK - 1) / C3_TK), (unsigned)((ny + 1 + C3_TJ - 1) / C3_TJ),
               (unsigned)(3 * nx + 1 + (with_cells ? nx : 0)));
 }
+// The same space with pz consecutive planes per block: blockIdx.z covers the
+// planes pz*blockIdx.z .. +pz-1, so a thread can issue the loads of all its
+// planes before it uses any of them.
+__host__ inline dim3 grid_faces_multi(int nx, int ny, int nz, bool with_cells, int pz) {
+  const int planes = 3 * nx + 1 + (with_cells ? nx : 0);
+  return dim3((unsigned)((nz + 1 + C3_TK - 1) / C3_TK), (unsigned)((ny + 1 + C3_TJ - 1) / C3_TJ),
+              (unsigned)((planes + pz - 1) / pz));
+}
+// element of plane z (of `planes` in all) for this thread, as locate
+__device__ __forceinline__ int locate_plane(const FaceSpace& s, int z, int planes, long long* f, int* i, int* j,
+                                            int* k) {
+  if (z >= planes) return -1;
+  int a;
+  if (z < s.nx + 1) a = 0;
+  else if ((z -= s.nx + 1) < s.nx) a = 1;
+  else if ((z -= s.nx) < s.nx) a = 2;
+  else { z -= s.nx; a = 3; }
+  const int n1 = s.ny + (a == 1), n2 = s.nz + (a == 2);
+  const int jj = (int)(blockIdx.y * C3_TJ + (threadIdx.x >> 5)), kk = (int)(blockIdx.x * C3_TK + (threadIdx.x & 31));
+  if (jj >= n1 || kk >= n2) return -1;
+  *i = z;
+  *j = jj;
+  *k = kk;
+  *f = ((long long)z * n1 + jj) * n2 + kk;
+  return a;
+}
+
 __device__ __forceinline__ int locate(const FaceSpace& s, long long* f, int* i, int* j, int* k) {
   int z = (int)blockIdx.z, a;
   if (z < s.nx + 1) a = 0;

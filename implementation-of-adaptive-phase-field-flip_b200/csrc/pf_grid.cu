@@ -76,19 +76,32 @@ struct ForceArgs {
   float dt;
 };
 
-// vel_star = vel; vel += g*dt; walls/obstacles zeroed (pfflip/sim.py:176-177, :270-285)
+// vel_star = vel; vel += g*dt; walls/obstacles zeroed (pfflip/sim.py:176-177, :270-285).
+// FP_PZ planes per thread, their loads issued before any store.
+constexpr int FP_PZ = 4;
+
 __global__ void __launch_bounds__(C3_NT) k_save_force(const __grid_constant__ ForceArgs a) {
   const FaceSpace& S = a.s;
-  {
-    long long f;
-    int i, j, k;
-    const int ax = locate(S, &f, &i, &j, &k);
-    if (ax < 0) return;
-    float v = a.vel[ax][f];
-    if (a.vstar[ax]) a.vstar[ax][f] = v;
-    if (a.g[ax] != 0.f) v += a.g[ax] * a.dt;
-    if (boundary_face(ax, i, j, k, S.nx, S.ny, S.nz) || solid_face(a.solid, ax, i, j, k, S.nx, S.ny, S.nz)) v = 0.f;
-    a.vel[ax][f] = v;
+  const int planes = 3 * S.nx + 1;
+  long long f[FP_PZ];
+  int ax[FP_PZ], ii[FP_PZ], jj[FP_PZ], kk[FP_PZ];
+  float v[FP_PZ];
+#pragma unroll
+  for (int p = 0; p < FP_PZ; ++p) {
+    ax[p] = locate_plane(S, (int)blockIdx.z * FP_PZ + p, planes, &f[p], &ii[p], &jj[p], &kk[p]);
+    v[p] = ax[p] >= 0 ? a.vel[ax[p]][f[p]] : 0.f;
+  }
+#pragma unroll
+  for (int p = 0; p < FP_PZ; ++p) {
+    const int x = ax[p];
+    if (x < 0) continue;
+    float u = v[p];
+    if (a.vstar[x]) a.vstar[x][f[p]] = u;
+    if (a.g[x] != 0.f) u += a.g[x] * a.dt;
+    if (boundary_face(x, ii[p], jj[p], kk[p], S.nx, S.ny, S.nz) ||
+        solid_face(a.solid, x, ii[p], jj[p], kk[p], S.nx, S.ny, S.nz))
+      u = 0.f;
+    a.vel[x][f[p]] = u;
   }
 }
 
@@ -128,22 +141,33 @@ struct ProjArgs {
   float dx, dt;
 };
 
-// pfflip/kernels.py:366-387
+// pfflip/kernels.py:366-387, FP_PZ planes per thread with their loads first
 __global__ void __launch_bounds__(C3_NT) k_project(const __grid_constant__ ProjArgs a) {
   const FaceSpace& S = a.s;
-  {
-    long long f;
+  const int planes = 3 * S.nx + 1;
+  long long f[FP_PZ];
+  int ax[FP_PZ];
+  float bc[FP_PZ], pi[FP_PZ], pm[FP_PZ], u[FP_PZ];
+#pragma unroll
+  for (int p = 0; p < FP_PZ; ++p) {
     int i, j, k;
-    const int ax = locate(S, &f, &i, &j, &k);
-    if (ax < 0) return;
-    const float bc = a.beta[ax][f];
-    if (bc == 0.f) return;
-    const int im = i - (ax == 0), jm = j - (ax == 1), km = k - (ax == 2);
-    if (im < 0 || jm < 0 || km < 0) return;
-    if (i >= S.nx || j >= S.ny || k >= S.nz) return;
-    const float pi = a.p[((long long)i * S.ny + j) * S.nz + k];
-    const float pm = a.p[((long long)im * S.ny + jm) * S.nz + km];
-    a.vel[ax][f] -= a.dt * bc * (pi - pm) / a.dx;
+    ax[p] = locate_plane(S, (int)blockIdx.z * FP_PZ + p, planes, &f[p], &i, &j, &k);
+    bc[p] = 0.f;
+    if (ax[p] < 0) continue;
+    const int im = i - (ax[p] == 0), jm = j - (ax[p] == 1), km = k - (ax[p] == 2);
+    if (im < 0 || jm < 0 || km < 0 || i >= S.nx || j >= S.ny || k >= S.nz) {  // wall faces: beta is 0
+      ax[p] = -1;
+      continue;
+    }
+    bc[p] = a.beta[ax[p]][f[p]];
+    pi[p] = a.p[((long long)i * S.ny + j) * S.nz + k];
+    pm[p] = a.p[((long long)im * S.ny + jm) * S.nz + km];
+    u[p] = a.vel[ax[p]][f[p]];
+  }
+#pragma unroll
+  for (int p = 0; p < FP_PZ; ++p) {
+    if (ax[p] < 0 || bc[p] == 0.f) continue;
+    a.vel[ax[p]][f[p]] = u[p] - a.dt * bc[p] * (pi[p] - pm[p]) / a.dx;
   }
 }
 
@@ -378,7 +402,7 @@ int pf_save_and_force(const pf_grid* g, float* vel_x, float* vel_y, float* vel_z
   a.solid = solid;
   a.g[0] = gx; a.g[1] = gy; a.g[2] = gz;
   a.dt = dt;
-  k_save_force<<<grid_faces(g->nx, g->ny, g->nz, false), C3_NT, 0, S(stream)>>>(a);
+  k_save_force<<<grid_faces_multi(g->nx, g->ny, g->nz, false, FP_PZ), C3_NT, 0, S(stream)>>>(a);
   PF_LAUNCHED();
   return PF_OK;
 }
@@ -405,7 +429,7 @@ int pf_project(const pf_grid* g, const float* p, const float* beta_x, const floa
   a.vel[0] = vel_x; a.vel[1] = vel_y; a.vel[2] = vel_z;
   a.dx = g->dx;
   a.dt = dt;
-  k_project<<<grid_faces(g->nx, g->ny, g->nz, false), C3_NT, 0, S(stream)>>>(a);
+  k_project<<<grid_faces_multi(g->nx, g->ny, g->nz, false, FP_PZ), C3_NT, 0, S(stream)>>>(a);
   PF_LAUNCHED();
   return PF_OK;
 }
