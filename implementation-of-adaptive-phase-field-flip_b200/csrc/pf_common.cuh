@@ -78,6 +78,28 @@ template <class T> __device__ __forceinline__ float roundT(float v) {
 }
 template <class T> __device__ __forceinline__ void stT(T* p, float v) { Store<T>::st(p, v); }
 
+// ---------------------------------------------------------------- particle sort keys
+// linear index of the cell floor(x/dx) (IEEE binary32 division, clamped to the grid)
+__device__ __forceinline__ int cell_key(float x, float y, float z, float dx, int nx, int ny, int nz) {
+  int i = (int)floorf(x / dx), j = (int)floorf(y / dx), k = (int)floorf(z / dx);
+  i = min(max(i, 0), nx - 1);
+  j = min(max(j, 0), ny - 1);
+  k = min(max(k, 0), nz - 1);
+  return (i * ny + j) * nz + k;
+}
+
+// warp-aggregated atomicAdd(&ctr[key], 1) over the lanes in `active`: returns this lane's slot
+__device__ __forceinline__ int agg_inc(int* ctr, int key, unsigned active) {
+  const unsigned grp = __match_any_sync(active, key);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(grp) - 1;
+  const int rank = __popc(grp & ((1u << lane) - 1u));
+  int base = 0;
+  if (lane == leader) base = atomicAdd(ctr + key, __popc(grp));
+  base = __shfl_sync(grp, base, leader);
+  return base + rank;
+}
+
 // ---------------------------------------------------------------- index helpers
 struct Dim3i {
   int n0, n1, n2;

@@ -1,44 +1,26 @@
 // Stable counting sort of particles by cell (no reference counterpart: the
 // reference keeps particles in seeding order, pfflip/scenes.py:23-29).
 //
-//   1. keys + histogram: key = linear index of the cell floor(x/dx) (IEEE
-//      binary32 division, clamped), counts by warp-aggregated atomics
+//   1. keys + ranks: key = linear index of the cell floor(x/dx) (IEEE binary32
+//      division, clamped); a warp-aggregated atomicAdd on the cell's count
+//      returns each particle's arrival rank within its cell
 //   2. exclusive scan of the counts -> cell_start (3-phase block scan)
-//   3. scatter: slot = cursor[key]++ (warp-aggregated), perm[slot] = p
-//   4. per-cell order fix: atomics leave the slots of one cell in arrival
-//      order; one warp per cell ranks the original indices so each cell's
-//      segment is ascending, which is exactly a stable sort; sorted keys are
-//      written here
+//   3. scatter: perm[cell_start[key] + rank] = p (no atomics)
+//   4. per-cell order fix: the ranks of one cell follow arrival order; one
+//      warp per cell ranks the original indices so each cell's segment is
+//      ascending, which is exactly a stable sort; sorted keys are written here
 //   5. gather of the two float4 particle streams through perm
 //
-// Bytes per particle: 16 (pos) + 4 (key) in pass 1, 8 in pass 3, 12 in pass 4,
-// 4 + 32 + 32 in pass 5, plus 8 per cell for the scan.
+// Bytes per particle: 16 (pos) + 8 (key, rank) in pass 1, 8 + 4 in pass 3,
+// 12 in pass 4, 4 + 32 + 32 in pass 5, plus 8 per cell for the scan.
 #include "pf_common.cuh"
 
 namespace pf {
 
-__device__ __forceinline__ int cell_key(float x, float y, float z, float dx, int nx, int ny, int nz) {
-  int i = (int)floorf(x / dx), j = (int)floorf(y / dx), k = (int)floorf(z / dx);
-  i = min(max(i, 0), nx - 1);
-  j = min(max(j, 0), ny - 1);
-  k = min(max(k, 0), nz - 1);
-  return (i * ny + j) * nz + k;
-}
-
-// warp-aggregated atomicAdd(&ctr[key], 1): returns this lane's slot
-__device__ __forceinline__ int agg_inc(int* ctr, int key, unsigned active) {
-  const unsigned grp = __match_any_sync(active, key);
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(grp) - 1;
-  const int rank = __popc(grp & ((1u << lane) - 1u));
-  int base = 0;
-  if (lane == leader) base = atomicAdd(ctr + key, __popc(grp));
-  base = __shfl_sync(grp, base, leader);
-  return base + rank;
-}
-
-__global__ void k_keys_hist(long long n, const float4* __restrict__ pos, float dx, int nx, int ny, int nz,
-                            int* __restrict__ keys, int* __restrict__ counts) {
+// pass 1: key and arrival rank within the cell (ranks of one cell are
+// 0..count-1 in some order), counts into `counts`
+__global__ void k_keys_rank(long long n, const float4* __restrict__ pos, float dx, int nx, int ny, int nz,
+                            int2* __restrict__ key_rank, int* __restrict__ counts) {
   for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
     const long long p = base + threadIdx.x;
     const bool in = p < n;
@@ -46,8 +28,7 @@ __global__ void k_keys_hist(long long n, const float4* __restrict__ pos, float d
     if (!in) continue;
     const float4 q = __ldg(pos + p);
     const int key = cell_key(q.x, q.y, q.z, dx, nx, ny, nz);
-    keys[p] = key;
-    agg_inc(counts, key, active);
+    key_rank[p] = make_int2(key, agg_inc(counts, key, active));
   }
 }
 
@@ -114,25 +95,19 @@ __global__ void __launch_bounds__(SCAN_NT) k_scan_sums(int m, int* __restrict__ 
   }
 }
 
-__global__ void k_scan_add(long long n, int* __restrict__ a, const int* __restrict__ sums, int* __restrict__ cursor) {
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-    const int v = a[e] + sums[e / SCAN_TILE];
-    a[e] = v;
-    if (cursor) cursor[e] = v;
-  }
+__global__ void k_scan_add(long long n, int* __restrict__ a, const int* __restrict__ sums) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    a[e] += sums[e / SCAN_TILE];
 }
 
 // ---------------------------------------------------------------- scatter + order fix
-__global__ void k_scatter(long long n, const int* __restrict__ keys, int* __restrict__ cursor,
-                          int* __restrict__ perm) {
-  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
-    const long long p = base + threadIdx.x;
-    const bool in = p < n;
-    const unsigned active = __ballot_sync(0xffffffffu, in);
-    if (!in) continue;
-    const int key = keys[p];
-    const int slot = agg_inc(cursor, key, active);
-    perm[slot] = (int)p;
+// pass 3: perm[start[key] + rank] = p; the slots of one cell are then in
+// arrival order, which k_fix_order turns into index order
+__global__ void k_scatter_rank(long long n, const int2* __restrict__ key_rank, const int* __restrict__ start,
+                               int* __restrict__ perm) {
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    const int2 kr = key_rank[p];
+    perm[start[kr.x] + kr.y] = (int)p;
   }
 }
 
@@ -218,40 +193,26 @@ size_t pf_sort_workspace_bytes(const pf_grid* g, int64_t n) {
   if (!g) return 0;
   const long long nc = (long long)g->nx * g->ny * g->nz;
   const long long tiles = (nc + 1 + SCAN_TILE - 1) / SCAN_TILE;
-  return (size_t)(4 * n + 4 * (nc + 1) + 4 * (tiles + 1) + 256);
+  return (size_t)(8 * n + 4 * (tiles + 1) + 256);
 }
 
-int pf_sort_particles(const pf_grid* g, int64_t n, const float* pos4_in, const float* vel4_in, float* pos4_out,
-                      float* vel4_out, int32_t* keys_out, int32_t* perm_out, int32_t* cell_start, void* workspace,
-                      size_t workspace_bytes, void* stream) {
-  PF_REQUIRE(g && n >= 0 && pos4_in && vel4_in && pos4_out && vel4_out && keys_out && perm_out && cell_start,
-             "null argument");
-  PF_REQUIRE(g->nx > 0 && g->ny > 0 && g->nz > 0 && g->dx > 0.f, "bad grid");
-  PF_REQUIRE((long long)g->nx * g->ny * g->nz < (1LL << 31) && n < (1LL << 31), "too large for int32 indices");
-  PF_REQUIRE(aligned16(pos4_in) && aligned16(vel4_in) && aligned16(pos4_out) && aligned16(vel4_out),
-             "particle streams must be 16-byte aligned");
-  PF_REQUIRE(pos4_in != pos4_out && vel4_in != vel4_out, "sort output must not alias its input");
-  PF_REQUIRE(workspace && workspace_bytes >= pf_sort_workspace_bytes(g, n), "workspace too small");
-  cudaStream_t s = S(stream);
+}  // extern "C"
+
+namespace {
+// passes 2-5, after (key, rank) per particle and the counts in cell_start
+int sort_from_keys(const pf_grid* g, int64_t n, const int2* key_rank, int* sums, const float* pos4_in,
+                   const float* vel4_in, float* pos4_out, float* vel4_out, int32_t* keys_out, int32_t* perm_out,
+                   int32_t* cell_start, cudaStream_t s) {
   const long long nc = (long long)g->nx * g->ny * g->nz;
   const long long tiles = (nc + 1 + SCAN_TILE - 1) / SCAN_TILE;
-  int* keys_tmp = reinterpret_cast<int*>(workspace);
-  int* cursor = keys_tmp + n;
-  int* sums = cursor + (nc + 1);
-  PF_CUDA_TRY(cudaMemsetAsync(cell_start, 0, sizeof(int) * (nc + 1), s));
-  if (n > 0) {
-    k_keys_hist<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, reinterpret_cast<const float4*>(pos4_in), g->dx,
-                                                               g->nx, g->ny, g->nz, keys_tmp, cell_start);
-    PF_LAUNCHED();
-  }
   k_scan_tiles<<<(int)tiles, SCAN_NT, 0, s>>>(nc + 1, cell_start, sums);
   PF_LAUNCHED();
   k_scan_sums<<<1, SCAN_NT, 0, s>>>((int)tiles, sums);
   PF_LAUNCHED();
-  k_scan_add<<<grid_for(nc + 1, 256, kNumSMs * 16), 256, 0, s>>>(nc + 1, cell_start, sums, cursor);
+  k_scan_add<<<grid_for(nc + 1, 256, kNumSMs * 16), 256, 0, s>>>(nc + 1, cell_start, sums);
   PF_LAUNCHED();
   if (n == 0) return PF_OK;
-  k_scatter<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, keys_tmp, cursor, perm_out);
+  k_scatter_rank<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, key_rank, cell_start, perm_out);
   PF_LAUNCHED();
   k_fix_order<<<grid_for(nc, 256, 1 << 20), 256, 0, s>>>((int)nc, cell_start, perm_out, keys_out);
   PF_LAUNCHED();
@@ -261,6 +222,53 @@ int pf_sort_particles(const pf_grid* g, int64_t n, const float* pos4_in, const f
                                                           reinterpret_cast<float4*>(vel4_out));
   PF_LAUNCHED();
   return PF_OK;
+}
+
+// pass 1: clear the counts, then (key, rank) per particle
+int keys_and_ranks(const pf_grid* g, int64_t n, const float* pos4_in, int2* key_rank, int32_t* cell_start,
+                   cudaStream_t s) {
+  const long long nc = (long long)g->nx * g->ny * g->nz;
+  PF_CUDA_TRY(cudaMemsetAsync(cell_start, 0, sizeof(int) * (nc + 1), s));
+  if (n > 0) {
+    k_keys_rank<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, reinterpret_cast<const float4*>(pos4_in), g->dx,
+                                                               g->nx, g->ny, g->nz, key_rank, cell_start);
+    PF_LAUNCHED();
+  }
+  return PF_OK;
+}
+
+// the argument checks every entry point shares
+int check_sort_args(const pf_grid* g, int64_t n, const float* pos4_in, const float* vel4_in, const float* pos4_out,
+                    const float* vel4_out, const int32_t* keys_out, const int32_t* perm_out,
+                    const int32_t* cell_start) {
+  PF_REQUIRE(g && n >= 0 && pos4_in && vel4_in && pos4_out && vel4_out && keys_out && perm_out && cell_start,
+             "null argument");
+  PF_REQUIRE(g->nx > 0 && g->ny > 0 && g->nz > 0 && g->dx > 0.f, "bad grid");
+  PF_REQUIRE((long long)g->nx * g->ny * g->nz < (1LL << 31) && n < (1LL << 31), "too large for int32 indices");
+  PF_REQUIRE(aligned16(pos4_in) && aligned16(vel4_in) && aligned16(pos4_out) && aligned16(vel4_out),
+             "particle streams must be 16-byte aligned");
+  PF_REQUIRE(pos4_in != pos4_out && vel4_in != vel4_out, "sort output must not alias its input");
+  return PF_OK;
+}
+}  // namespace
+
+extern "C" {
+
+// workspace layout: (key, rank) per particle (8n bytes), then the scan's
+// per-tile sums
+int pf_sort_particles(const pf_grid* g, int64_t n, const float* pos4_in, const float* vel4_in, float* pos4_out,
+                      float* vel4_out, int32_t* keys_out, int32_t* perm_out, int32_t* cell_start, void* workspace,
+                      size_t workspace_bytes, void* stream) {
+  int rc = check_sort_args(g, n, pos4_in, vel4_in, pos4_out, vel4_out, keys_out, perm_out, cell_start);
+  if (rc != PF_OK) return rc;
+  PF_REQUIRE(workspace && workspace_bytes >= pf_sort_workspace_bytes(g, n) && aligned16(workspace),
+             "workspace too small or not 16-byte aligned");
+  cudaStream_t s = S(stream);
+  int2* key_rank = reinterpret_cast<int2*>(workspace);
+  rc = keys_and_ranks(g, n, pos4_in, key_rank, cell_start, s);
+  if (rc != PF_OK) return rc;
+  return sort_from_keys(g, n, key_rank, reinterpret_cast<int*>(key_rank + n), pos4_in, vel4_in, pos4_out, vel4_out,
+                        keys_out, perm_out, cell_start, s);
 }
 
 }  // extern "C"
@@ -307,75 +315,25 @@ static int static_tile_sums(int** out) {
   return PF_OK;
 }
 
-// pass 1: key and arrival rank within the cell (ranks of one cell are
-// 0..count-1 in some order), counts into `counts`
-__global__ void k_keys_rank(long long n, const float4* __restrict__ pos, float dx, int nx, int ny, int nz,
-                            int2* __restrict__ key_rank, int* __restrict__ counts) {
-  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
-    const long long p = base + threadIdx.x;
-    const bool in = p < n;
-    const unsigned active = __ballot_sync(0xffffffffu, in);
-    if (!in) continue;
-    const float4 q = __ldg(pos + p);
-    const int key = cell_key(q.x, q.y, q.z, dx, nx, ny, nz);
-    key_rank[p] = make_int2(key, agg_inc(counts, key, active));
-  }
-}
-
-// pass 3: perm[start[key] + rank] = p; the slots of one cell are then in
-// arrival order, which k_fix_order turns into index order
-__global__ void k_scatter_rank(long long n, const int2* __restrict__ key_rank, const int* __restrict__ start,
-                               int* __restrict__ perm) {
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-    const int2 kr = key_rank[p];
-    perm[start[kr.x] + kr.y] = (int)p;
-  }
-}
-
 }  // namespace pf
 
 extern "C" int pf_sort_particles_static(const pf_grid* g, int64_t n, const float* pos4_in, const float* vel4_in,
                                         float* pos4_out, float* vel4_out, int32_t* keys_out, int32_t* perm_out,
                                         int32_t* cell_start, void* stream) {
-  PF_REQUIRE(g && n >= 0 && pos4_in && vel4_in && pos4_out && vel4_out && keys_out && perm_out && cell_start,
-             "null argument");
-  PF_REQUIRE(g->nx > 0 && g->ny > 0 && g->nz > 0 && g->dx > 0.f, "bad grid");
+  int rc = check_sort_args(g, n, pos4_in, vel4_in, pos4_out, vel4_out, keys_out, perm_out, cell_start);
+  if (rc != PF_OK) return rc;
   const long long nc = (long long)g->nx * g->ny * g->nz;
   PF_REQUIRE(nc <= kStaticMaxCells,
              "grid of %lld cells exceeds the %lld cells (512^3) the static scratch covers; use pf_sort_particles "
              "with a workspace",
              nc, kStaticMaxCells);
-  PF_REQUIRE(n < (1LL << 31), "too large for int32 indices");
-  PF_REQUIRE(aligned16(pos4_in) && aligned16(vel4_in) && aligned16(pos4_out) && aligned16(vel4_out),
-             "particle streams must be 16-byte aligned");
-  PF_REQUIRE(pos4_in != pos4_out && vel4_in != vel4_out, "sort output must not alias its input");
   int* sums = nullptr;
-  const int rc = static_tile_sums(&sums);
+  rc = static_tile_sums(&sums);
   if (rc != PF_OK) return rc;
   cudaStream_t s = S(stream);
-  const long long tiles = (nc + 1 + SCAN_TILE - 1) / SCAN_TILE;
   int2* key_rank = reinterpret_cast<int2*>(pos4_out);
-  PF_CUDA_TRY(cudaMemsetAsync(cell_start, 0, sizeof(int) * (nc + 1), s));
-  if (n > 0) {
-    k_keys_rank<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, reinterpret_cast<const float4*>(pos4_in), g->dx,
-                                                               g->nx, g->ny, g->nz, key_rank, cell_start);
-    PF_LAUNCHED();
-  }
-  k_scan_tiles<<<(int)tiles, SCAN_NT, 0, s>>>(nc + 1, cell_start, sums);
-  PF_LAUNCHED();
-  k_scan_sums<<<1, SCAN_NT, 0, s>>>((int)tiles, sums);
-  PF_LAUNCHED();
-  k_scan_add<<<grid_for(nc + 1, 256, kNumSMs * 16), 256, 0, s>>>(nc + 1, cell_start, sums, nullptr);
-  PF_LAUNCHED();
-  if (n == 0) return PF_OK;
-  k_scatter_rank<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, key_rank, cell_start, perm_out);
-  PF_LAUNCHED();
-  k_fix_order<<<grid_for(nc, 256, 1 << 20), 256, 0, s>>>((int)nc, cell_start, perm_out, keys_out);
-  PF_LAUNCHED();
-  k_gather<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, perm_out, reinterpret_cast<const float4*>(pos4_in),
-                                                          reinterpret_cast<const float4*>(vel4_in),
-                                                          reinterpret_cast<float4*>(pos4_out),
-                                                          reinterpret_cast<float4*>(vel4_out));
-  PF_LAUNCHED();
-  return PF_OK;
+  rc = keys_and_ranks(g, n, pos4_in, key_rank, cell_start, s);
+  if (rc != PF_OK) return rc;
+  return sort_from_keys(g, n, key_rank, sums, pos4_in, vel4_in, pos4_out, vel4_out, keys_out, perm_out, cell_start,
+                        s);
 }

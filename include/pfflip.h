@@ -88,7 +88,8 @@ uint64_t pf_launch_count(void);
  *   out: pos4_out, vel4_out (sorted), keys_out[n] (sorted keys), perm_out[n]
  *        (perm_out[t] = input slot of the t-th sorted particle), cell_start
  *        [nx*ny*nz + 1] (particles of cell c are [cell_start[c], cell_start[c+1]))
- *   pos4_out/vel4_out must not alias the inputs. */
+ *   pos4_out/vel4_out must not alias the inputs; the workspace
+ *   (pf_sort_workspace_bytes) is 16-byte aligned. */
 size_t pf_sort_workspace_bytes(const pf_grid* g, int64_t n);
 int pf_sort_particles(const pf_grid* g, int64_t n, const float* pos4_in, const float* vel4_in, float* pos4_out,
                       float* vel4_out, int32_t* keys_out, int32_t* perm_out, int32_t* cell_start, void* workspace,
@@ -184,11 +185,12 @@ int pf_g2p_advect(const pf_grid* g, int64_t n, float* pos4, float* vel4, const f
                   float alpha_liquid, float alpha_air, float dt, const float lo[3], const float hi[3],
                   int32_t do_g2p, int32_t do_advect, void* stream);
 
-/* The same pass reading the face fields through k-paired copies built in the
- * caller's workspace (pf_g2p_workspace_bytes, 256-byte aligned): per face,
- * (u[k], u[k+1], u*[k], u*[k+1]) and (vel_liq[k], vel_liq[k+1]).  A sample
- * then takes four row loads instead of eight gathers; every tap value and sum
- * is the one pf_g2p_advect forms.  Same arguments and results otherwise. */
+/* The same pass reading the face fields through (j, k) quads built in the
+ * caller's workspace (pf_g2p_workspace_bytes, 256-byte aligned): per face of
+ * u, u* and vel_liq, (v[j][k], v[j][k+1], v[j+1][k], v[j+1][k+1]).  A
+ * trilinear sample then takes two 16-byte loads instead of eight gathers;
+ * every tap value is the one pf_g2p_advect reads (sums within rounding).
+ * Same arguments and results otherwise. */
 size_t pf_g2p_workspace_bytes(const pf_grid* g);
 int pf_g2p_advect_packed(const pf_grid* g, int64_t n, float* pos4, float* vel4, const float* vel_x,
                          const float* vel_y, const float* vel_z, const float* vstar_x, const float* vstar_y,

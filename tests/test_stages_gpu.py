@@ -52,12 +52,34 @@ def gpu_sort(pos, vel, res, dx):
     return keys[:n].cpu().numpy(), perm[:n].cpu().numpy(), start.cpu().numpy(), po[:n].cpu().numpy(), vo[:n].cpu().numpy()
 
 
-@pytest.mark.parametrize("case", ["random", "dam_break", "clustered", "walls", "empty", "one_cell"])
+def _near_faces(rng, res, dx, n):
+    """Coordinates on and within 4 ulps of the cell faces k * dx (binary32),
+    where x * (1/dx) and x / dx can round to different sides of an integer."""
+    out = np.empty((n, 3), np.float32)
+    for a in range(3):
+        f = (rng.integers(0, res[a] + 1, n).astype(np.float32) * np.float32(dx)).astype(np.float32)
+        steps = rng.integers(-4, 5, n)
+        for s in range(-4, 5):
+            m = steps == s
+            v = f[m]
+            for _ in range(abs(s)):
+                v = np.nextafter(v, np.float32(np.inf if s > 0 else -np.inf)).astype(np.float32)
+            f[m] = v
+        out[:, a] = f
+    return out
+
+
+@pytest.mark.parametrize("case", ["random", "dam_break", "clustered", "walls", "empty", "one_cell", "faces",
+                                  "faces_odd_dx"])
 def test_sort_bit_exact(case):
     rng = np.random.default_rng(11)
     res, dx = (24, 20, 36), np.float32(1 / 24)
+    if case == "faces_odd_dx":
+        dx = np.float32(0.0137)
     L = np.array(res, np.float64) * float(dx)
-    if case == "random":
+    if case.startswith("faces"):  # keys of coordinates at the cell faces follow the division
+        pos = _near_faces(rng, res, dx, 120_000)
+    elif case == "random":
         pos = (rng.random((200_003, 3)) * L).astype(np.float32)
     elif case == "dam_break":
         cfg = Config(res=(32,) * 3, dx=1 / 32, ppc=8)
@@ -272,9 +294,9 @@ def test_step_matches_oracle_dam_break_32():
 
 @pytest.mark.parametrize("flags", [(1, 1), (1, 0), (0, 1)])
 def test_g2p_packed_matches_unpaired(flags):
-    """pf_g2p_advect_packed reads k-paired copies of the fields; every tap and
-    sum is the unpaired kernel's, so results agree to rounding (FMA contraction
-    may differ): 4 ulps of the largest value."""
+    """pf_g2p_advect_packed reads (j, k) quads of the fields; every tap is the
+    unpaired kernel's, so results agree to rounding (the sums associate
+    differently): 4 ulps of the largest value."""
     do_g2p, do_adv = flags
     res = (24, 20, 36)
     dx = np.float32(1 / 24)
