@@ -121,8 +121,14 @@ __device__ __forceinline__ void push_out_of_solids(const int* __restrict__ solid
   }
   if (best <= 1.0e8f) {
     const float off = (best + 0.5f) * dx * (float)bsg;
-    x[bax] = x[bax] + off;
-    if ((float)bsg * v[bax] < 0.f) v[bax] = 0.f;
+    // x[bax] and v[bax] through compile-time indices: a runtime index would
+    // keep x and v in local memory for the whole particle loop
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (c != bax) continue;
+      x[c] = x[c] + off;
+      if ((float)bsg * v[c] < 0.f) v[c] = 0.f;
+    }
   }
 }
 

@@ -85,8 +85,9 @@ def test_hierarchy_matches_oracle_bitwise():
             assert np.array_equal(getattr(L, name).numpy(), o.level_array(lv, name)), (lv, name)
 
 
-# ragged tiles; the second and third take 8-plane tiles
-@pytest.mark.parametrize("res", [(24, 40, 36), (136, 44, 36), (162, 68, 64)])
+# ragged tiles; (70, 40, 36) takes 8-plane tiles (the last one 6 planes deep),
+# the two largest 6-plane tiles (the last of 136 planes 4 deep)
+@pytest.mark.parametrize("res", [(24, 40, 36), (70, 40, 36), (136, 44, 36), (162, 68, 64)])
 @pytest.mark.parametrize("stencil", ["reference", "flux"])
 def test_smoother_matches_oracle(stencil, res):
     rng = np.random.default_rng(5)
