@@ -25,6 +25,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include <cooperative_groups.h>
@@ -588,9 +589,17 @@ __device__ __forceinline__ void sweep_mean_finish(const SweepArgs<T, TB>& a, dou
   }
 }
 
+// Programmatic dependent launch: a sweep is launched so that it may start
+// while the kernel before it finishes.  Until griddepcontrol.wait returns (all
+// prerequisite grids complete, their writes visible) it touches only its own
+// shared memory and the face coefficients, which no kernel of a solve writes;
+// it lets the next kernel launch as soon as all of its own CTAs are resident.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 template <int TI, int NT>
 __global__ void __launch_bounds__(NT) k_rb_tile_tma(const __grid_constant__ TileMaps maps, SweepArgs<float, float> a) {
-  if (is_done(a.st)) return;
+  grid_dep_launch();
   using D = TmaDims<TI>;
   extern __shared__ __align__(128) unsigned char tsm_raw[];
   unsigned char* tsm = tsm_raw + ((128u - (smem_u32(tsm_raw) & 127u)) & 127u);
@@ -610,22 +619,34 @@ __global__ void __launch_bounds__(NT) k_rb_tile_tma(const __grid_constant__ Tile
   const int hn1 = n1 >> 1, hn2 = n2 >> 1;
   const bool load_p = !a.zero_in;
 
+  const int x = k0 - TM_X0;
   if (tid == 0) {
     s_fail = 0;
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    const unsigned bytes = 4u * (unsigned)((load_p ? D::PN : 0) + D::BN + D::XN + D::YN + D::ZN);
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+    // the faces first, while the previous kernel may still run
+    const unsigned fbytes = 4u * (unsigned)(D::XN + D::YN + D::ZN);
+    asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(fbytes)
                  : "memory");
-    const int x = k0 - TM_X0;
-    if (load_p) tma_load_3d(sP, &maps.p, x, j0 - 2, i0 - 2, bar);
-    tma_load_3d(sB, &maps.b, x, j0 - 1, i0 - 1, bar);
     tma_load_3d(sX, &maps.x, x, j0 - 1, i0 - 1, bar);
     tma_load_3d(sY, &maps.y, x, j0 - 1, i0 - 1, bar);
     tma_load_3d(sZ, &maps.z, x, j0 - 1, i0 - 1, bar);
   }
   if (!load_p)
     for (int e = tid; e < D::PN; e += NT) sP[e] = 0.f;
+  grid_dep_wait();
+  const bool done = is_done(a.st);
+  if (tid == 0) {
+    // p and b come from the previous kernels; a finished solve loads nothing
+    // more and only lets the face copies land before the CTA leaves
+    const unsigned bytes = done ? 0u : 4u * (unsigned)((load_p ? D::PN : 0) + D::BN);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    if (!done) {
+      if (load_p) tma_load_3d(sP, &maps.p, x, j0 - 2, i0 - 2, bar);
+      tma_load_3d(sB, &maps.b, x, j0 - 1, i0 - 1, bar);
+    }
+  }
   __syncthreads();  // barrier initialised before anyone waits on it
   {
     unsigned it = 0;
@@ -647,6 +668,7 @@ __global__ void __launch_bounds__(NT) k_rb_tile_tma(const __grid_constant__ Tile
     }
     return;
   }
+  if (done) return;
   double msum = 0.0;
   tma_tile_sweep<TI, NT, float, float>(sP, sB, sX, sY, sZ, a, k0, j0, i0, msum);
   sweep_mean_finish<NT>(a, msum, sred);
@@ -2302,6 +2324,25 @@ bool tma_maps16(pf_mg_plan* P, int lv, const T* p_in, const TB* b, const LV<T>& 
   }
 }
 
+// launch that may overlap the end of the kernel before it on the stream
+// (programmatic dependent launch); the kernel must call griddepcontrol.wait
+// before it reads anything an earlier kernel writes
+template <class... KArgs, class... Args>
+cudaError_t launch_overlapped(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 template <class T, class TB>
 int launch_sweep(pf_mg_plan* P, int lv, const T* p_in, bool zero_in, T* p_out, const TB* b, const float* b_scale,
                  const LV<T>& V, const T* pc, float pc_scale, int first_color, bool mean, bool use_state,
@@ -2331,7 +2372,7 @@ int launch_sweep(pf_mg_plan* P, int lv, const T* p_in, bool zero_in, T* p_out, c
     // per cell); 2% faster per solve than 8-plane tiles at two CTAs per SM
     if (P->use_tma && L.nx >= 128 && tma_maps<6, T, TB>(P, lv, p_in, b, b_scale, V, &maps)) {
       const dim3 g6(grid.x, grid.y, (L.nx + 5) / 6);
-      k_rb_tile_tma<6, 512><<<g6, 512, TmaDims<6>::SMEM, s>>>(maps, a);
+      PF_CUDA_TRY(launch_overlapped(k_rb_tile_tma<6, 512>, g6, dim3(512), TmaDims<6>::SMEM, s, maps, a));
       PF_LAUNCHED();
       return PF_OK;
     }
@@ -2340,12 +2381,12 @@ int launch_sweep(pf_mg_plan* P, int lv, const T* p_in, bool zero_in, T* p_out, c
     // of 256 CTAs, which six-plane tiles (352 CTAs) do not beat
     if (P->use_tma && L.nx >= 64 && tma_maps<8, T, TB>(P, lv, p_in, b, b_scale, V, &maps)) {
       const dim3 g8(grid.x, grid.y, (L.nx + 7) / 8);
-      k_rb_tile_tma<8, 512><<<g8, 512, TmaDims<8>::SMEM, s>>>(maps, a);
+      PF_CUDA_TRY(launch_overlapped(k_rb_tile_tma<8, 512>, g8, dim3(512), TmaDims<8>::SMEM, s, maps, a));
       PF_LAUNCHED();
       return PF_OK;
     }
     if (P->use_tma && tma_maps<TI, T, TB>(P, lv, p_in, b, b_scale, V, &maps)) {
-      k_rb_tile_tma<TI, SW_NT><<<grid, SW_NT, TmaDims<TI>::SMEM, s>>>(maps, a);
+      PF_CUDA_TRY(launch_overlapped(k_rb_tile_tma<TI, SW_NT>, grid, dim3(SW_NT), TmaDims<TI>::SMEM, s, maps, a));
       PF_LAUNCHED();
       return PF_OK;
     }
