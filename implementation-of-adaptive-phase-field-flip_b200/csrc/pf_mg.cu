@@ -697,7 +697,7 @@ template <int TI, bool B32> struct Tma16Dims {
 
 template <int TI, int NT, class T, class TB>
 __global__ void __launch_bounds__(NT) k_rb_tile_tma16(const __grid_constant__ TileMaps maps, SweepArgs<T, TB> a) {
-  if (is_done(a.st)) return;
+  grid_dep_launch();  // launched like k_rb_tile_tma: faces before the wait, p and b after it
   constexpr bool B32 = std::is_same<TB, float>::value;
   using D = TmaDims<TI>;
   using E = Tma16Dims<TI, B32>;
@@ -715,20 +715,28 @@ __global__ void __launch_bounds__(NT) k_rb_tile_tma16(const __grid_constant__ Ti
   const int k0 = blockIdx.x * SW_TK, j0 = blockIdx.y * SW_TJ, i0 = blockIdx.z * TI;
   const int tid = threadIdx.x;
   const bool load_p = !a.zero_in;
+  const int x16 = k0 - TM16_X0, xb = B32 ? k0 - TM_X0 : k0 - TM16_X0;
   if (tid == 0) {
     s_fail = 0;
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    const unsigned bytes =
-        (unsigned)((load_p ? E::P16N * 2 : 0) + E::BN * E::BES + (E::XN + E::YN + E::ZN) * 2);
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+    const unsigned fbytes = (unsigned)((E::XN + E::YN + E::ZN) * 2);
+    asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(fbytes)
                  : "memory");
-    const int x16 = k0 - TM16_X0, xb = B32 ? k0 - TM_X0 : k0 - TM16_X0;
-    if (load_p) tma_load_3d(sP16, &maps.p, x16, j0 - 2, i0 - 2, bar);
-    tma_load_3d(sB, &maps.b, xb, j0 - 1, i0 - 1, bar);
     tma_load_3d(sX, &maps.x, x16, j0 - 1, i0 - 1, bar);
     tma_load_3d(sY, &maps.y, x16, j0 - 1, i0 - 1, bar);
     tma_load_3d(sZ, &maps.z, x16, j0 - 1, i0 - 1, bar);
+  }
+  grid_dep_wait();
+  const bool done = is_done(a.st);
+  if (tid == 0) {
+    const unsigned bytes = done ? 0u : (unsigned)((load_p ? E::P16N * 2 : 0) + E::BN * E::BES);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    if (!done) {
+      if (load_p) tma_load_3d(sP16, &maps.p, x16, j0 - 2, i0 - 2, bar);
+      tma_load_3d(sB, &maps.b, xb, j0 - 1, i0 - 1, bar);
+    }
   }
   __syncthreads();  // barrier initialised before anyone waits on it
   {
@@ -751,6 +759,7 @@ __global__ void __launch_bounds__(NT) k_rb_tile_tma16(const __grid_constant__ Ti
     }
     return;
   }
+  if (done) return;
   for (int e = tid; e < D::PN; e += NT) {  // p: 16-bit rows from k0 - 8 -> fp32 rows from k0 - 4
     const int row = e / TM_W, c = e - row * TM_W;
     sP[e] = load_p ? ldT(sP16 + row * TM16_W + c + (TM16_X0 - TM_X0)) : 0.f;
@@ -2396,13 +2405,14 @@ int launch_sweep(pf_mg_plan* P, int lv, const T* p_in, bool zero_in, T* p_out, c
     constexpr bool B32 = std::is_same<TB, float>::value;
     if (P->use_tma && L.nx >= 128 && tma_maps16<8, T, TB>(P, lv, p_in, b, V, &maps)) {
       const dim3 g8(grid.x, grid.y, (L.nx + 7) / 8);
-      k_rb_tile_tma16<8, 512, T, TB><<<g8, 512, Tma16Dims<8, B32>::SMEM, s>>>(maps, a);
+      PF_CUDA_TRY(launch_overlapped(k_rb_tile_tma16<8, 512, T, TB>, g8, dim3(512), Tma16Dims<8, B32>::SMEM, s, maps,
+                                    a));
       PF_LAUNCHED();
       return PF_OK;
     }
     if (P->use_tma && tma_maps16<TI, T, TB>(P, lv, p_in, b, V, &maps)) {
-      k_rb_tile_tma16<TI, SW_NT, T, TB>
-          <<<grid, SW_NT, Tma16Dims<TI, std::is_same<TB, float>::value>::SMEM, s>>>(maps, a);
+      PF_CUDA_TRY(launch_overlapped(k_rb_tile_tma16<TI, SW_NT, T, TB>, grid, dim3(SW_NT), Tma16Dims<TI, B32>::SMEM, s,
+                                    maps, a));
       PF_LAUNCHED();
       return PF_OK;
     }
