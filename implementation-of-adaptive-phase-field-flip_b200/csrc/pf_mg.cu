@@ -592,14 +592,14 @@ __device__ __forceinline__ void sweep_mean_finish(const SweepArgs<T, TB>& a, dou
 // Programmatic dependent launch: a sweep is launched so that it may start
 // while the kernel before it finishes.  Until griddepcontrol.wait returns (all
 // prerequisite grids complete, their writes visible) it touches only its own
-// shared memory and the face coefficients, which no kernel of a solve writes;
-// it lets the next kernel launch as soon as all of its own CTAs are resident.
+// shared memory and the face coefficients, which no kernel of a solve writes.
+// Once its tile has landed it lets the next kernel launch (which then starts
+// when every CTA of this one has done so or exited).
 __device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 template <int TI, int NT>
 __global__ void __launch_bounds__(NT) k_rb_tile_tma(const __grid_constant__ TileMaps maps, SweepArgs<float, float> a) {
-  grid_dep_launch();
   using D = TmaDims<TI>;
   extern __shared__ __align__(128) unsigned char tsm_raw[];
   unsigned char* tsm = tsm_raw + ((128u - (smem_u32(tsm_raw) & 127u)) & 127u);
@@ -668,6 +668,7 @@ __global__ void __launch_bounds__(NT) k_rb_tile_tma(const __grid_constant__ Tile
     }
     return;
   }
+  grid_dep_launch();  // staged: the next kernel may start its own staging now
   if (done) return;
   double msum = 0.0;
   tma_tile_sweep<TI, NT, float, float>(sP, sB, sX, sY, sZ, a, k0, j0, i0, msum);
@@ -697,7 +698,7 @@ template <int TI, bool B32> struct Tma16Dims {
 
 template <int TI, int NT, class T, class TB>
 __global__ void __launch_bounds__(NT) k_rb_tile_tma16(const __grid_constant__ TileMaps maps, SweepArgs<T, TB> a) {
-  grid_dep_launch();  // launched like k_rb_tile_tma: faces before the wait, p and b after it
+  // launched like k_rb_tile_tma: faces before the wait, p and b after it
   constexpr bool B32 = std::is_same<TB, float>::value;
   using D = TmaDims<TI>;
   using E = Tma16Dims<TI, B32>;
@@ -759,6 +760,7 @@ __global__ void __launch_bounds__(NT) k_rb_tile_tma16(const __grid_constant__ Ti
     }
     return;
   }
+  grid_dep_launch();
   if (done) return;
   for (int e = tid; e < D::PN; e += NT) {  // p: 16-bit rows from k0 - 8 -> fp32 rows from k0 - 4
     const int row = e / TM_W, c = e - row * TM_W;
