@@ -315,21 +315,27 @@ __global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(const __grid_const
     const bool flip = pstate == 0;
     Frame fx;
     if (flip && (a.do_g2p || a.do_advect)) make_frame(x, a.inv_dx, a.nx, a.ny, a.nz, fx);
+    float pic[3];  // I(u) at x: an air particle's first RK3 stage samples the same field there
     if (a.do_g2p && flip) {
       const float alpha = liquid ? a.a_liq : a.a_air;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         Rows r;
         rows_of(fx, c, a.ny, a.nz, r);
-        float delta, pic;
-        sample_g2p_packed(a.qu[c], a.qs[c], r, delta, pic);
-        v[c] = alpha * (v[c] + delta) + (1.f - alpha) * pic;
+        float delta;
+        sample_g2p_packed(a.qu[c], a.qs[c], r, delta, pic[c]);
+        v[c] = alpha * (v[c] + delta) + (1.f - alpha) * pic[c];
       }
     }
     if (a.do_advect) {
       if (flip) {
         float k1[3], k2[3], k3[3], y[3];
-        sample_vel_packed(a, liquid, fx, k1);
+        if (a.do_g2p && !liquid) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) k1[c] = pic[c];
+        } else {
+          sample_vel_packed(a, liquid, fx, k1);
+        }
         const float h1 = 0.5f * a.dt, h2 = 0.75f * a.dt;
 #pragma unroll
         for (int c = 0; c < 3; ++c) y[c] = x[c] + h1 * k1[c];
