@@ -925,7 +925,8 @@ __device__ __forceinline__ void bt_relax(R* P, const float* B, const float* X, c
     sum += bzu * q5;
     res = (R)B[e] - (d * pv - sum);
   }
-  P[e] = pv + omega * res / d;
+  if constexpr (std::is_same<R, float>::value) P[e] = pv + __fdividef(omega * res, d);  // as gs_update
+  else P[e] = pv + omega * res / d;
 }
 
 // `sweeps` red-black sweeps of a coarsest level of at most 64 cells with an
@@ -1555,7 +1556,7 @@ __device__ __forceinline__ void bc_relax(const DLv& L, int li, int j, int k, flo
     sum += bzu * q5;
     res = L.B[e] - (d * pv - sum);
   }
-  P[e] = pv + omega * res / d;
+  P[e] = pv + __fdividef(omega * res, d);  // as gs_update
 }
 
 // the cells of `color` in this CTA's slab (n2 even: two cells per k pair);
