@@ -313,7 +313,7 @@ def run_ours(args):
         traffic = None
         if "bytes_per_particle" in tr:
             traffic = tr["bytes_per_particle"] * n + tr.get("bytes_per_cell", 0.0) * ncell
-        roof = {"kernel": {"p2g": "k_p2g", "g2p_advect": "k_g2p_advect"}[dom], "bound": "hbm", "achieved": ach,
+        roof = {"kernel": {"p2g": "k_p2g", "g2p_advect": "k_g2p_advect_packed"}[dom], "bound": "hbm", "achieved": ach,
                 "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
                 "algorithmic_bytes_per_launch": ab, "traffic": traffic}
     for k, v in per_stage.items():
