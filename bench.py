@@ -230,37 +230,74 @@ def run_reference(args):
     return 0
 
 
+# ---------------------------------------------------------------- ranks
+class Ranks:
+    """Process-group plumbing of a run over N ranks (one process per GPU,
+    launched by torch.distributed.run).  The step does not shard, so the ranks
+    exchange no data: they meet at barriers around the timed region and reduce
+    one number, the elapsed time (max over ranks).  Every rank takes the same
+    collective calls in the same order.  ``backend`` is "nccl" on GPUs; the
+    CPU tests drive the same code with "gloo"."""
+
+    def __init__(self, backend, device):
+        import torch
+
+        self.torch = torch
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.device = device
+        self.dist = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            kw = {"device_id": device} if backend == "nccl" else {}
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300), **kw)
+            self.dist = dist
+
+    @property
+    def root(self):
+        return self.rank == 0
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+        if self.device.type == "cuda":
+            self.torch.cuda.synchronize(self.device)
+
+    def max(self, x):
+        """max of x over the ranks (x itself on one rank)"""
+        if self.dist is None:
+            return float(x)
+        t = self.torch.tensor([float(x)], dtype=self.torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def job_rate(world, ms_per_step_max):
+    """whole-job steps/s of N replicas whose slowest rank took ms_per_step_max"""
+    return world * 1000.0 / ms_per_step_max
+
+
 # ---------------------------------------------------------------- GPU legs
 def run_ours(args):
     import torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    ranks = Ranks("nccl", torch.device("cuda", local))
+    world, rank = ranks.world, ranks.rank
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     from pfflip import Simulator
     from pfflip import _native as N
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     cfg = workload_cfg(args)
     dt = fixed_dt(cfg.dx)
@@ -295,7 +332,7 @@ def run_ours(args):
     stages = sim.stage_times(reset=True)
     sim.enable_stage_timing(False)
     iters = float(np.mean([r["pcg_iter"] for r in recs]))
-    value = world * 1000.0 / ms
+    value = job_rate(world, ms)
 
     # roofline of the dominant single-kernel stage
     peak, peak_kind = peaks()
@@ -352,7 +389,7 @@ def run_ours(args):
         f1.record(stream)
         barrier()
         ems = max_over_ranks(f0.elapsed_time(f1) / args.steps)
-        line["e2e"] = {"value": world * 1000.0 / ems, "unit": UNIT, "h2d_bytes_per_step": int(n * 28),
+        line["e2e"] = {"value": job_rate(world, ems), "unit": UNIT, "h2d_bytes_per_step": int(n * 28),
                        "d2h_bytes_per_step": int(n * 24),
                        "api": "Simulator.set_particles(pinned host) + step(dt) + read_particles(pinned host)"}
 
@@ -386,9 +423,7 @@ def run_ours(args):
                                           f"({n:,} particles), all host threads"}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 
