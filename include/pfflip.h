@@ -47,7 +47,7 @@ extern "C" {
 #define PF_ERR_NONFINITE 3     /* a NaN/Inf appeared in the CG residual */
 #define PF_ERR_NOT_CONVERGED 4 /* tolerance not met within max_iter (results still valid) */
 #define PF_ERR_WORKSPACE 5     /* workspace too small */
-#define PF_ERR_UNSUPPORTED 6   /* option not supported by this build */
+#define PF_ERR_UNSUPPORTED 6   /* option not supported by this library */
 
 #define PF_FLAG_LIQUID 1u
 #define PF_PSTATE_SHIFT 1

@@ -274,8 +274,9 @@ def test_g2p_advect_match_oracle():
 
 
 def test_step_matches_oracle_dam_break_32():
-    """BASELINE config 1 (32^3 dam break, 8 ppc, fixed dt): three full steps on
-    the GPU and on the oracle from the same seeded particles."""
+    """The 32^3 dam break with 8 ppc at a fixed dt, the reference's CPU-sized
+    case: three full steps on the GPU and on the oracle from the same seeded
+    particles."""
     cfg = Config(res=(32, 32, 32), dx=1 / 32, ppc=8, seed=42, droplets=False, pcg_tol=1e-6)
     dt = 0.5 * cfg.dx / np.sqrt(2 * 9.81 * 0.6)
     sim = Simulator(cfg)
