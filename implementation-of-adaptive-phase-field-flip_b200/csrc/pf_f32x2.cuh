@@ -20,16 +20,8 @@ __device__ __forceinline__ f2 f2_make(float x, float y) {
   return r;
 }
 __device__ __forceinline__ f2 f2_bcast(float x) { return f2_make(x, x); }
-__device__ __forceinline__ float f2_x(f2 a) {
-  float x, y;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(a.v));
-  return x;
-}
-__device__ __forceinline__ float f2_y(f2 a) {
-  float x, y;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(a.v));
-  return y;
-}
+__device__ __forceinline__ float f2_x(f2 a) { return __uint_as_float((unsigned)a.v); }
+__device__ __forceinline__ float f2_y(f2 a) { return __uint_as_float((unsigned)(a.v >> 32)); }
 __device__ __forceinline__ void f2_split(f2 a, float& x, float& y) {
   asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(a.v));
 }

@@ -60,7 +60,6 @@ enum {
 static_assert(CNT_MAX <= PF_MG_COUNTERS, "counters");
 
 constexpr int RED_NT = 256;
-constexpr int RED_MAX_BLOCKS = 2 * kNumSMs * 4;  // 1184 partials per reduction
 constexpr int64_t kPartials = 1 << 16;  // >= CTAs of any one reduction (sweep tiles up to 512^3)
 
 __device__ __forceinline__ bool is_done(const MGState* st) { return st != nullptr && st->done != 0; }
@@ -615,11 +614,8 @@ __global__ void __launch_bounds__(NT) k_rb_tile_tma(const __grid_constant__ Tile
   __shared__ double sred[40];
   __shared__ int s_fail;
 
-  const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
   const int k0 = blockIdx.x * SW_TK, j0 = blockIdx.y * SW_TJ, i0 = blockIdx.z * TI;
   const int tid = threadIdx.x;
-  const long long sI = (long long)n1 * n2;
-  const int hn1 = n1 >> 1, hn2 = n2 >> 1;
   const bool load_p = !a.zero_in;
 
   const int x = k0 - TM_X0;
@@ -3000,7 +2996,6 @@ int pf_mg_plan_create(const pf_mg_desc* desc, pf_mg_plan** out) {
     if (P->sms <= 0) P->sms = kNumSMs;
   }
   for (int lv = 0; lv < desc->nlev; ++lv) {
-    const pf_mg_level& L = desc->lev[lv];
     P->lp_scale[lv] = std::ldexp(desc->coef_scale > 0.f ? desc->coef_scale : 1.f, -2 * lv);
   }
   {
@@ -3127,7 +3122,6 @@ int pf_apply_A(const pf_grid* g, const float* p, const float* bx, const float* b
                const float* diag, float* out, int32_t stencil, void* stream) {
   PF_REQUIRE(g && p && bx && by && bz && out, "null argument");
   PF_REQUIRE(stencil == PF_STENCIL_REFERENCE || stencil == PF_STENCIL_FLUX, "bad stencil");
-  const long long n = (long long)g->nx * g->ny * g->nz;
   k_apply_A<<<grid_cells(g->nx, g->ny, g->nz), C3_NT, 0, S(stream)>>>(g->nx, g->ny, g->nz, p, bx, by, bz, diag, out,
                                                                       stencil == PF_STENCIL_FLUX ? 1 : 0);
   PF_LAUNCHED();
