@@ -182,7 +182,7 @@ class Simulator:
         self.step_index = 0
         self.stats: list[dict] = []
         self._marks = None  # per-stage CUDA events when stage timing is on
-        self._g2p_ws = None  # k-paired face fields of the G2P/advection pass
+        self._g2p_ws = None  # (j, k) quads of the face fields read by the G2P/advection pass
 
         self.px = ParticleField(self, "pos")
         self.pv = ParticleField(self, "vel")
