@@ -64,7 +64,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
-    ap.add_argument("--solve-oracle", action="store_true", help="also solve the 128^3 problem with the FP64 oracle")
+    ap.add_argument("--no-solve-oracle", action="store_true",
+                    help="skip the FP64 CG oracle (solved to 1e-12) that the solve leg's errors are measured against")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the step-accuracy leg (phi, pressure, divergence of the FP32/FP16/BF16 step vs FP64)")
     ap.add_argument("--solve-only", action="store_true", help="only the standalone solve leg (prints its JSON)")
     ap.add_argument("--solve-variants", default="fp32_flux,fp16_flux,bf16_flux,fp32_reference",
                     help="comma list of precision_stencil variants for the solve leg")
@@ -74,8 +77,8 @@ def parse():
     ap.add_argument("--adjoint-only", action="store_true", help="only the gradient leg (prints its JSON)")
     ap.add_argument("--adjoint-res", type=int, default=64)
     ap.add_argument("--adjoint-steps", type=int, default=20)
-    ap.add_argument("--adjoint-fd", action="store_true",
-                    help="check the gradient against FP64 central differences of the CPU oracle (slow)")
+    ap.add_argument("--no-adjoint-fd", action="store_true",
+                    help="skip the check of the gradient against FP64 central differences of the CPU oracle")
     ap.add_argument("--rt", action="store_true",
                     help="also time the Rayleigh-Taylor workload (256^3, 8 ppc, 16 modes), FP32 and 16-bit hierarchy")
     ap.add_argument("--rt-only", action="store_true", help="only the Rayleigh-Taylor leg (prints its JSON)")
@@ -216,18 +219,31 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     steps = max(1, min(args.steps, 2))
     warm = min(args.warmup, 1)
+    probe = warp_probe()
     times = cpu_oracle_steps(cfg, pos, vel, pt, warm + steps, threads)[warm:]
     v = len(times) / sum(times)
     sample = (f"{len(times)} full oracle steps (after {warm} warm-up) of the {args.res}^3/{args.ppc}ppc dam break, "
-              f"{len(pos):,} particles; reference runtime NVIDIA Warp unavailable, so the CPU restatement of the "
-              f"reference kernels (oracle/pf_oracle.hpp) runs in its place")
+              f"{len(pos):,} particles; reference runtime NVIDIA Warp unavailable on this box ({probe}), so the "
+              f"CPU restatement of the reference kernels (oracle/pf_oracle.hpp) runs in its place")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": len(times), "warmup": warm, "ms_per_step": 1000.0 / v, "higher_is_better": True,
             "dtype": "f32", "data": "synthetic", "config": {"workload": f"dam_break {args.res}^3 {args.ppc}ppc"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "warp_probe": probe}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def warp_probe():
+    """Whether the reference's runtime (NVIDIA Warp, warp-lang) imports here:
+    the exception's one-line text, or its version.  The reference package
+    itself is not on this machine either way, so the oracle port stands in."""
+    try:
+        import warp  # noqa: F401
+    except Exception as e:  # ModuleNotFoundError on these boxes
+        return f"import warp: {type(e).__name__}: {e}"
+    return f"import warp: ok, version {getattr(warp, '__version__', '?')}"
 
 
 # ---------------------------------------------------------------- ranks
@@ -403,6 +419,12 @@ def run_ours(args):
         torch.cuda.empty_cache()
         line["mixed"] = mixed_leg(args, pos, vel, pt, dt, ms)
 
+    # accuracy of the FP32 and 16-bit-hierarchy steps against the FP64 oracle
+    if not args.no_accuracy and rank == 0:
+        sim = None
+        torch.cuda.empty_cache()
+        line["accuracy"] = accuracy_leg(args, pos, vel, pt, dt)
+
     # differentiable asteroid: gradient of |phi_T - phi*|^2 with respect to v0
     if not args.no_adjoint and rank == 0:
         sim = None
@@ -439,10 +461,20 @@ def solve_leg(args):
     dev = lambda a: DeviceArray(torch.from_numpy(a).cuda())  # noqa: E731
     out = {"workload": f"standalone solve {r}^3, 1000:1, tol 1e-6, pre=post=3"}
     ref64 = None
-    if args.solve_oracle:
+    if not args.no_solve_oracle:
         from oracle import oracle as O
 
-        ref64, _, _ = O.fp64_reference_solve(bx, by, bz, b.astype(np.float64), tol=1e-12)
+        O.set_threads(os.cpu_count() or 1)
+        t0 = time.perf_counter()
+        b64 = b.astype(np.float64)
+        ref64, it64, rel64 = O.fp64_reference_solve(bx, by, bz, b64, tol=1e-12)
+        f64 = [a.astype(np.float64) for a in (bx, by, bz)]
+        diag64 = O.compute_diag(*f64)
+        out["fp64_oracle"] = {"tol": 1e-12, "iters": it64, "rel": rel64, "cpu_s": time.perf_counter() - t0,
+                              "threads": O.get_threads(),
+                              "errors": "err_vs_fp64 = max|x - mean(x) - x64| / max|x64| (x64 zero-mean); "
+                                        "residual_fp64 = max|b - A x| / max|b| in binary64 (A x = the "
+                                        "divergence a projection with x leaves, times -dx/dt)"}
     for var in args.solve_variants.split(","):
         prec, stencil = var.split("_")
         s = MGPCG((r, r, r), "cuda", pre=3, post=3, precision=prec, stencil=stencil, use_graphs=not args.no_graphs)
@@ -462,6 +494,8 @@ def solve_leg(args):
         rec = {"ms": float(np.median(ts)), "iters": it, "rel": rel, "converged": rel < 1e-6}
         if ref64 is not None:
             xv = x.numpy().astype(np.float64)
+            ax64 = O.apply_A(xv, *f64, diag64, dtype=np.float64, stencil="flux")
+            rec["residual_fp64"] = float(np.abs(b64 - ax64).max() / np.abs(b64).max())
             xv -= xv.mean()
             rec["err_vs_fp64"] = float(np.abs(xv - ref64).max() / np.abs(ref64).max())
         out[f"{prec}_{stencil}"] = rec
@@ -493,6 +527,105 @@ def mixed_leg(args, pos, vel, pt, dt, ms_fp32):
         del sim
         torch.cuda.empty_cache()
     return res
+
+
+def accuracy_leg(args, pos, vel, pt, dt, warm_steps=2):
+    """Errors of one step of the workload against the binary64 oracle, for the
+    plain FP32 step and the FP16/BF16-hierarchy steps.
+
+    The particle state after ``warm_steps`` FP32 steps from the seed (so the
+    velocities are not zero) is the input of every variant and of the oracle.
+    Each variant runs the step's stages on the GPU: sort/P2G, phi/beta,
+    u* + gravity, RHS, hierarchy, MG-PCG at the step's tolerance, projection.
+    The oracle (pf_oracle.hpp in binary64, 1e-12 CG) is fed the same inputs:
+
+    * phi: binary64 P2G + eq. (7) from the same particles (the hierarchy's
+      precision does not reach phi, so one value serves every variant);
+    * pressure: the binary64 solve of the GPU's own system (its beta and RHS),
+      error after mean removal, relative to max|p64| -- the solver's error;
+      and against the all-binary64 pipeline from the particles;
+    * divergence: max|div u|/dx after the GPU projection, next to the oracle's
+      binary64 projection of the same velocities with p64, and the relative
+      error of the projected face velocities."""
+    import dataclasses
+
+    import torch
+
+    from oracle import oracle as O
+    from pfflip import Simulator
+
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    t_cpu = 0.0
+    cfg32 = workload_cfg(args, precision="fp32")
+    sim = Simulator(cfg32)
+    sim.set_particles(pos, vel, pt)
+    for _ in range(warm_steps):
+        sim.step(dt)
+    hp, hv, ht = sim.px.numpy(), sim.pv.numpy(), sim.ptype.numpy()
+    del sim
+    torch.cuda.empty_cache()
+
+    c64 = dataclasses.replace(cfg32, pcg_tol=1e-12, pcg_max_iter=1000)
+    t0 = time.perf_counter()
+    o = O.OracleSim(c64, dtype=np.float64, nthreads=threads, stencil="flux")
+    o.set_particles(hp, hv, ht)
+    o._p2g()
+    o._phase_field_and_coefficients()
+    o._save_vel_star()
+    o._add_forces(dt)
+    it_pipe, rel_pipe = o._pressure_solve(dt)
+    p_pipe = o.pressure - o.pressure.mean()
+    phi64 = o.phi_cell.copy()
+    t_cpu += time.perf_counter() - t0
+
+    out = {"workload": f"one step of dam_break {args.res}^3 {args.ppc}ppc after {warm_steps} FP32 steps, "
+                       f"pcg_tol {args.tol}",
+           "oracle": "pf_oracle.hpp binary64, CG to 1e-12", "threads": threads}
+    p64 = None
+    for prec in ("fp32", "fp16", "bf16"):
+        sim = Simulator(workload_cfg(args, precision=prec))
+        sim.set_particles(hp, hv, ht)
+        sim._p2g()
+        sim._phase_field_and_coefficients()
+        sim._add_forces(dt, save_vel_star=True)
+        it, rel = sim._pressure_solve(dt)
+        p = sim.pressure.numpy().astype(np.float64)
+        p -= p.mean()
+        if p64 is None:  # the GPU's system is the same for every variant: solve it once
+            t0 = time.perf_counter()
+            beta = [b.numpy().astype(np.float64) for b in sim.beta]
+            rhs = sim.rhs.numpy().astype(np.float64)
+            p64, it64, rel64 = O.fp64_reference_solve(*beta, rhs, tol=1e-12, max_iter=1000)
+            vel_pre = [v.numpy().astype(np.float64) for v in sim.vel]
+            o.pressure[...] = p64
+            for ax in range(3):
+                o.vel[ax][...] = vel_pre[ax]
+                o.beta[ax][...] = beta[ax]
+            o._project(dt)
+            div64 = o._max_divergence()
+            vel64 = [v.copy() for v in o.vel]
+            t_cpu += time.perf_counter() - t0
+            phi = sim.phi_cell.numpy().astype(np.float64)
+            out["phi_err_vs_fp64"] = float(np.abs(phi - phi64).max())
+            out["phi_note"] = "max|phi - phi64| (phi in [0, 1]); P2G and eq. (7) are FP32 in every variant"
+            out["pressure_fp64_system"] = {"iters": it64, "rel": rel64, "max_div_after_projection": div64}
+            out["pressure_fp64_pipeline"] = {"iters": it_pipe, "rel": rel_pipe}
+        sim._project(dt)
+        div = sim._max_divergence()
+        vp = [v.numpy().astype(np.float64) for v in sim.vel]
+        vscale = max(np.abs(v).max() for v in vel64)
+        out[prec] = {
+            "pcg_iter": it, "pcg_rel": rel,
+            "pressure_err_vs_fp64": float(np.abs(p - p64).max() / np.abs(p64).max()),
+            "pressure_err_vs_fp64_pipeline": float(np.abs(p - p_pipe).max() / np.abs(p_pipe).max()),
+            "max_div_after_projection": div,
+            "velocity_err_vs_fp64_projection": float(max(np.abs(a - b).max() for a, b in zip(vp, vel64)) / vscale),
+        }
+        del sim
+        torch.cuda.empty_cache()
+    out["cpu_s"] = t_cpu
+    return out
 
 
 def rt_leg(args):
@@ -598,7 +731,7 @@ def adjoint_leg(args):
            "backward_ms_per_step": bwd_ms / steps,
            "adjoint_solve_iters_mean": float(np.mean([it for it, _ in solves])),
            "adjoint_solve_rel_max": float(max(rel for _, rel in solves))}
-    if args.adjoint_fd:
+    if not args.no_adjoint_fd:
         from oracle import oracle as O
 
         fr = args.adjoint_fd_res or r

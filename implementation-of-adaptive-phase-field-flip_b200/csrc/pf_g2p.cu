@@ -189,6 +189,12 @@ __global__ void __launch_bounds__(256) k_g2p_advect(const __grid_constant__ G2PA
     V.x = v[0]; V.y = v[1]; V.z = v[2];
     a.pos[p] = P;
     a.vel[p] = V;
+    if (flip) vmax = fmaxf(vmax, sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+  }
+  if (a.max_speed) {  // uniform: every thread of the grid takes this branch or none does
+    __shared__ float sh[40];
+    vmax = block_max<256>(vmax, sh);
+    if (threadIdx.x == 0) atomic_max_nonneg(a.max_speed, vmax);
   }
 }
 
@@ -223,6 +229,7 @@ struct G2PPackedArgs {
   const float4* ql[3];
   const int* solid;
   int do_g2p, do_advect;
+  float* max_speed;  // NULL, or max |v| of the FLIP particles after the pass
 };
 
 __global__ void __launch_bounds__(C3_NT) k_pack_faces(FacePack fp) {
@@ -304,6 +311,7 @@ __device__ __forceinline__ void sample_vel_packed(const G2PPackedArgs& a, bool l
 }
 
 __global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(const __grid_constant__ G2PPackedArgs a) {
+  float vmax = 0.f;  // CFL speed of this thread's FLIP particles (pfflip/kernels.py:552-564)
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
     float4 P = a.pos[p];
     float4 V = a.vel[p];
@@ -371,6 +379,12 @@ __global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(const __grid_const
     V.x = v[0]; V.y = v[1]; V.z = v[2];
     a.pos[p] = P;
     a.vel[p] = V;
+    if (flip) vmax = fmaxf(vmax, sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+  }
+  if (a.max_speed) {  // uniform: every thread of the grid takes this branch or none does
+    __shared__ float sh[40];
+    vmax = block_max<256>(vmax, sh);
+    if (threadIdx.x == 0) atomic_max_nonneg(a.max_speed, vmax);
   }
 }
 
@@ -442,8 +456,8 @@ extern "C" int pf_g2p_advect_packed(const pf_grid* g, int64_t n, float* pos4, fl
                                     const float* vstar_y, const float* vstar_z, const float* vliq_x,
                                     const float* vliq_y, const float* vliq_z, const int32_t* solid,
                                     float alpha_liquid, float alpha_air, float dt, const float lo[3],
-                                    const float hi[3], int32_t do_g2p, int32_t do_advect, void* workspace,
-                                    size_t workspace_bytes, void* stream) {
+                                    const float hi[3], int32_t do_g2p, int32_t do_advect, float* max_speed,
+                                    void* workspace, size_t workspace_bytes, void* stream) {
   PF_REQUIRE(g && pos4 && vel4 && vel_x && vel_y && vel_z, "null argument");
   PF_REQUIRE(g->nx > 0 && g->ny > 0 && g->nz > 0, "bad grid");
   PF_REQUIRE(!do_g2p || (vstar_x && vstar_y && vstar_z), "u* fields required for G2P");
@@ -456,8 +470,9 @@ extern "C" int pf_g2p_advect_packed(const pf_grid* g, int64_t n, float* pos4, fl
                  (long long)(g->nx + 1) * g->ny * g->nz < (1LL << 31) &&
                  (long long)g->nx * (g->ny + 1) * g->nz < (1LL << 31),
              "face arrays must hold < 2^31 entries");
-  if (n <= 0) return PF_OK;
   cudaStream_t s = S(stream);
+  if (max_speed) PF_CUDA_TRY(cudaMemsetAsync(max_speed, 0, sizeof(float), s));
+  if (n <= 0) return PF_OK;
   unsigned char* ws = static_cast<unsigned char*>(workspace);
   FacePack fp;
   fp.s = make_space(g->nx, g->ny, g->nz);
@@ -493,6 +508,7 @@ extern "C" int pf_g2p_advect_packed(const pf_grid* g, int64_t n, float* pos4, fl
   a.solid = solid;
   a.do_g2p = do_g2p;
   a.do_advect = do_advect;
+  a.max_speed = max_speed;
   k_g2p_advect_packed<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(a);
   PF_LAUNCHED();
   return PF_OK;

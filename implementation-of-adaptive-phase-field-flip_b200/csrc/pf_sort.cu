@@ -13,6 +13,10 @@
 //
 // Bytes per particle: 16 (pos) + 8 (key, rank) in pass 1, 8 + 4 in pass 3,
 // 12 in pass 4, 4 + 32 + 32 in pass 5, plus 8 per cell for the scan.
+#include <cuda.h>
+
+#include <mutex>
+
 #include "pf_common.cuh"
 
 namespace pf {
@@ -237,6 +241,13 @@ int keys_and_ranks(const pf_grid* g, int64_t n, const float* pos4_in, int2* key_
   return PF_OK;
 }
 
+// true when the byte ranges [a, a + na) and [b, b + nb) share a byte
+bool ranges_overlap(const void* a, long long na, const void* b, long long nb) {
+  if (na <= 0 || nb <= 0) return false;
+  const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+  return x < y + (uintptr_t)nb && y < x + (uintptr_t)na;
+}
+
 // the argument checks every entry point shares
 int check_sort_args(const pf_grid* g, int64_t n, const float* pos4_in, const float* vel4_in, const float* pos4_out,
                     const float* vel4_out, const int32_t* keys_out, const int32_t* perm_out,
@@ -248,6 +259,24 @@ int check_sort_args(const pf_grid* g, int64_t n, const float* pos4_in, const flo
   PF_REQUIRE(aligned16(pos4_in) && aligned16(vel4_in) && aligned16(pos4_out) && aligned16(vel4_out),
              "particle streams must be 16-byte aligned");
   PF_REQUIRE(pos4_in != pos4_out && vel4_in != vel4_out, "sort output must not alias its input");
+  // every output must be disjoint from every other buffer of the call (the
+  // static variant also keeps its scratch in pos4_out for the whole call)
+  const long long nc = (long long)g->nx * g->ny * g->nz;
+  const struct {
+    const void* p;
+    long long bytes;
+    const char* name;
+    bool out;
+  } buf[7] = {{pos4_in, 16 * n, "pos4_in", false},   {vel4_in, 16 * n, "vel4_in", false},
+              {pos4_out, 16 * n, "pos4_out", true},  {vel4_out, 16 * n, "vel4_out", true},
+              {keys_out, 4 * n, "keys_out", true},   {perm_out, 4 * n, "perm_out", true},
+              {cell_start, 4 * (nc + 1), "cell_start", true}};
+  for (int a = 0; a < 7; ++a)
+    for (int b = a + 1; b < 7; ++b) {
+      if (!buf[a].out && !buf[b].out) continue;  // two inputs may share memory
+      PF_REQUIRE(!ranges_overlap(buf[a].p, buf[a].bytes, buf[b].p, buf[b].bytes), "%s overlaps %s", buf[a].name,
+                 buf[b].name);
+    }
   return PF_OK;
 }
 }  // namespace
@@ -263,6 +292,15 @@ int pf_sort_particles(const pf_grid* g, int64_t n, const float* pos4_in, const f
   if (rc != PF_OK) return rc;
   PF_REQUIRE(workspace && workspace_bytes >= pf_sort_workspace_bytes(g, n) && aligned16(workspace),
              "workspace too small or not 16-byte aligned");
+  {
+    const long long nc = (long long)g->nx * g->ny * g->nz, wb = (long long)workspace_bytes;
+    PF_REQUIRE(!ranges_overlap(workspace, wb, pos4_in, 16 * n) && !ranges_overlap(workspace, wb, vel4_in, 16 * n) &&
+                   !ranges_overlap(workspace, wb, pos4_out, 16 * n) &&
+                   !ranges_overlap(workspace, wb, vel4_out, 16 * n) &&
+                   !ranges_overlap(workspace, wb, keys_out, 4 * n) && !ranges_overlap(workspace, wb, perm_out, 4 * n) &&
+                   !ranges_overlap(workspace, wb, cell_start, 4 * (nc + 1)),
+               "workspace overlaps a particle stream or an output");
+  }
   cudaStream_t s = S(stream);
   int2* key_rank = reinterpret_cast<int2*>(workspace);
   rc = keys_and_ranks(g, n, pos4_in, key_rank, cell_start, s);
@@ -297,21 +335,73 @@ constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) int g_static_tile_sums[(kStaticTiles + 63) / 64 * 64];
 
-// device address of g_static_tile_sums, looked up once per device
-static std::atomic<int*> g_static_sums_addr[kMaxDevices];
+// Device address of g_static_tile_sums, looked up once per device and
+// context.  The address belongs to the context the module was loaded into:
+// after cudaDeviceReset (or with another context current on the same device)
+// the cached pointer would be stale, so the cache is keyed on the context's
+// process-unique id (cuCtxGetId, reached through the runtime's driver entry
+// point, so the library does not link the driver) and looked up again when
+// the current context changes.
+struct StaticSums {
+  unsigned long long ctx_id;  // 0: not looked up yet
+  int* addr;
+};
+static StaticSums g_static_sums[kMaxDevices];
+static std::mutex g_static_sums_mutex;
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+// id of the context current on this thread, 0 when none is current yet
+static int current_context_id(unsigned long long* id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  if (!get_current || !get_id) {
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = cudaDriverEntryPointSymbolNotFound;
+    PF_CUDA_TRY(cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1));
+    PF_CUDA_TRY(cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2));
+    if (q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2) {
+      set_error(PF_ERR_CUDA, "driver entry points cuCtxGetCurrent/cuCtxGetId unavailable");
+      return PF_ERR_CUDA;
+    }
+    get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+    get_id = reinterpret_cast<CtxGetIdFn>(f2);
+  }
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS) {
+    set_error(PF_ERR_CUDA, "cuCtxGetCurrent failed");
+    return PF_ERR_CUDA;
+  }
+  *id = 0;
+  if (ctx && get_id(ctx, id) != CUDA_SUCCESS) {
+    set_error(PF_ERR_CUDA, "cuCtxGetId failed");
+    return PF_ERR_CUDA;
+  }
+  return PF_OK;
+}
 
 static int static_tile_sums(int** out) {
   int dev = 0;
   PF_CUDA_TRY(cudaGetDevice(&dev));
   PF_REQUIRE(dev >= 0 && dev < kMaxDevices, "device ordinal %d beyond %d", dev, kMaxDevices);
-  int* a = g_static_sums_addr[dev].load(std::memory_order_acquire);
-  if (!a) {
+  std::lock_guard<std::mutex> lock(g_static_sums_mutex);
+  unsigned long long id = 0;
+  int rc = current_context_id(&id);
+  if (rc != PF_OK) return rc;
+  StaticSums& c = g_static_sums[dev];
+  if (id == 0 || c.ctx_id != id) {
+    // set-up for this device and context: the symbol lookup also creates the
+    // device's primary context when none is current yet
     void* sym = nullptr;
     PF_CUDA_TRY(cudaGetSymbolAddress(&sym, g_static_tile_sums));
-    a = static_cast<int*>(sym);
-    g_static_sums_addr[dev].store(a, std::memory_order_release);
+    rc = current_context_id(&id);
+    if (rc != PF_OK) return rc;
+    c.addr = static_cast<int*>(sym);
+    c.ctx_id = id;
   }
-  *out = a;
+  *out = c.addr;
   return PF_OK;
 }
 

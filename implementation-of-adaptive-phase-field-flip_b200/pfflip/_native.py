@@ -95,7 +95,7 @@ SIGNATURES = {
                                                                      C.POINTER(_F), _I32, _I32, _VP]),
     "pf_g2p_workspace_bytes": (C.c_size_t, [_G]),
     "pf_g2p_advect_packed": (C.c_int, [_G, _I64, _VP, _VP] + [_VP] * 9 + [_VP, _F, _F, _F, C.POINTER(_F),
-                                                                          C.POINTER(_F), _I32, _I32, _VP,
+                                                                          C.POINTER(_F), _I32, _I32, _VP, _VP,
                                                                           C.c_size_t, _VP]),
     "pf_particle_max_speed": (C.c_int, [_I64, _VP, _VP, _VP, _VP]),
     "pf_droplet_classify": (C.c_int, [_G, _I64, _VP, _VP, _VP, _VP, _F, _F, _F, _F, _F, C.c_uint32, _VP, _VP]),

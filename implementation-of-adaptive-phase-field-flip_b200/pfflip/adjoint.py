@@ -165,7 +165,7 @@ class DiffSim:
         for k in range(nsteps - 1, -1, -1):
             p0, v0 = states[k]
             s._pos4.copy_(p0)
-            s._fresh_sort = False
+            s._particles_changed()
             s._vel4.copy_(v0)
             self._grid_stages()
             # ga/gb are in the order of the arrays after the step, which is the
@@ -174,7 +174,7 @@ class DiffSim:
             self._step_adjoint(ga, gb, nxt_p, nxt_v)
             ga, gb = nxt_p, nxt_v
             s._pos4.copy_(p0)
-            s._fresh_sort = False
+            s._particles_changed()
             s._vel4.copy_(v0)
         # the arrays now hold the block's first state, in the order ga/gb use
         return self._to_ids(ga), self._to_ids(gb)

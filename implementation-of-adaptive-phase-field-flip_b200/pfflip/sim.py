@@ -107,7 +107,7 @@ class ParticleField:
 
     def assign(self, a):
         s, k = self._sim, self._kind
-        s._fresh_sort = False
+        s._particles_changed()
         ids = s._ids().long()
         t = torch.as_tensor(np.ascontiguousarray(np.asarray(a))).to(s.dev)
         if k in ("pos", "vel"):
@@ -169,6 +169,10 @@ class Simulator:
         # True only between set_particles (which sorts) and the next stage: the
         # step's own sort would then repeat it on the same particles
         self._fresh_sort = False
+        # True while _scal[2] holds the CFL speed of the particles as they are:
+        # the step's last particle pass leaves it there, and anything else that
+        # changes particle velocities or states clears this
+        self._vmax_valid = False
         self._pending_d2h = []  # (host lo, host hi, event) of read_particles' chunked downloads
         self._pos4 = self._vel4 = None
         self.droplet_stats = {"emitted": 0, "bubbles": 0, "merged": 0, "spray": 0}
@@ -256,6 +260,7 @@ class Simulator:
             self._drop_r.zero_()
         self._sort()
         self._fresh_sort = True
+        self._vmax_valid = False
 
     def read_particles(self, pos_out=None, vel_out=None):
         """Positions and velocities in the original order, copied into the given
@@ -390,11 +395,23 @@ class Simulator:
         return out
 
     # ------------------------------------------------------------------ step
+    def _particles_changed(self):
+        """Particle positions, velocities or states were written outside the
+        step: neither the last sort nor the last CFL speed describes them."""
+        self._fresh_sort = False
+        self._vmax_valid = False
+
     def dt_from_cfl(self) -> float:
+        """CFL time step (pfflip/sim.py:157-166).  Right after a step the FLIP
+        particles' max speed is already on the device (the step's last particle
+        pass reduces it); otherwise one pf_particle_max_speed pass computes it."""
         cfg = self.cfg
-        N.call("pf_particle_max_speed", self.n_particles, self._pos4.data_ptr(), self._vel4.data_ptr(),
-               self._scal.data_ptr(), N.stream())
-        vmax = float(self._scal[0].item())
+        if self._vmax_valid:
+            vmax = float(self._scal[2].item())
+        else:
+            N.call("pf_particle_max_speed", self.n_particles, self._pos4.data_ptr(), self._vel4.data_ptr(),
+                   self._scal.data_ptr(), N.stream())
+            vmax = float(self._scal[0].item())
         g = float(np.linalg.norm(cfg.gravity))
         vmax = max(vmax, math.sqrt(2.0 * g * cfg.dx) if g > 0 else 0.0, 1e-8)
         return float(np.clip(cfg.cfl * cfg.dx / vmax, cfg.dt_min, cfg.dt_max))
@@ -521,7 +538,7 @@ class Simulator:
         return lo, hi
 
     def _g2p_advect(self, dt, do_g2p, do_advect):
-        self._fresh_sort = False
+        self._particles_changed()
         lo, hi = self._bounds()
         cfg = self.cfg
         if self._g2p_ws is None:
@@ -531,7 +548,10 @@ class Simulator:
                self._vel4.data_ptr(), *(N.ptr(a) for a in self.vel), *(N.ptr(a) for a in self.vel_star),
                *(N.ptr(a) for a in self.vel_liq), N.ptr(self.solid) if self.has_solids else None,
                float(cfg.alpha_flip_liquid), float(cfg.alpha_flip_air), float(dt), lo, hi, int(do_g2p),
-               int(do_advect), self._g2p_ws.data_ptr(), self._g2p_ws.numel(), N.stream())
+               int(do_advect), self._scal.data_ptr() + 8 if do_advect else None, self._g2p_ws.data_ptr(),
+               self._g2p_ws.numel(), N.stream())
+        # after an advection pass the particles are as the step leaves them
+        self._vmax_valid = bool(do_advect)
 
     def _g2p(self):
         """eq. (11)-(12) FLIP/PIC update (pfflip/sim.py:316-327)."""
@@ -544,7 +564,7 @@ class Simulator:
 
     def _droplets(self, dt: float):
         """Escaped particles -> droplets, droplet dynamics (pfflip/sim.py:343-392)."""
-        self._fresh_sort = False
+        self._particles_changed()
         cfg = self.cfg
         if not cfg.droplets or self.n_particles == 0:
             return

@@ -88,7 +88,8 @@ uint64_t pf_launch_count(void);
  *   out: pos4_out, vel4_out (sorted), keys_out[n] (sorted keys), perm_out[n]
  *        (perm_out[t] = input slot of the t-th sorted particle), cell_start
  *        [nx*ny*nz + 1] (particles of cell c are [cell_start[c], cell_start[c+1]))
- *   pos4_out/vel4_out must not alias the inputs; the workspace
+ *   every output and the workspace must be disjoint from every other buffer
+ *   of the call (PF_ERR_ARG on any overlap); the workspace
  *   (pf_sort_workspace_bytes) is 16-byte aligned. */
 size_t pf_sort_workspace_bytes(const pf_grid* g, int64_t n);
 int pf_sort_particles(const pf_grid* g, int64_t n, const float* pos4_in, const float* vel4_in, float* pos4_out,
@@ -99,14 +100,18 @@ int pf_sort_particles(const pf_grid* g, int64_t n, const float* pos4_in, const f
  * For hosts that cannot hand over device scratch (all device memory fixed at
  * start-up, or a step that must not allocate).  Arguments, outputs and
  * results are those of pf_sort_particles.  The call allocates nothing:
- * per-particle scratch lives in pos4_out until the final gather, and the
- * scan's tile sums sit in a static device array of the library (131,328
- * bytes), which limits the grid to PF_SORT_STATIC_MAX_CELLS cells; larger
- * grids return PF_ERR_ARG.  cell_start is cleared on the stream each call;
- * nothing else needs to start at zero.  The first call on a device looks up
- * the array's address (cudaGetSymbolAddress): make it before any stream
- * capture.  All calls on a device share the array, so calls whose executions
- * overlap (different streams or host threads) race: order them. */
+ * per-particle scratch lives in pos4_out for the whole call (until the final
+ * gather writes the sorted positions there), and the scan's tile sums sit in
+ * a static device array of the library (131,328 bytes), which limits the grid
+ * to PF_SORT_STATIC_MAX_CELLS cells; larger grids return PF_ERR_ARG.  Every
+ * output must be disjoint from every other buffer of the call (checked:
+ * PF_ERR_ARG on any overlap).  cell_start is cleared on the stream each call;
+ * nothing else needs to start at zero.  The first call on a device, and the
+ * first after the current context changes (cudaDeviceReset, or another
+ * context made current), looks up the array's address in that context
+ * (cudaGetSymbolAddress): make it before any stream capture.  All calls on a
+ * device share the array, so calls whose executions overlap (different
+ * streams or host threads) race: order them. */
 #define PF_SORT_STATIC_MAX_CELLS 134217728LL /* 512^3 */
 int pf_sort_particles_static(const pf_grid* g, int64_t n, const float* pos4_in, const float* vel4_in,
                              float* pos4_out, float* vel4_out, int32_t* keys_out, int32_t* perm_out,
@@ -190,13 +195,18 @@ int pf_g2p_advect(const pf_grid* g, int64_t n, float* pos4, float* vel4, const f
  * u, u* and vel_liq, (v[j][k], v[j][k+1], v[j+1][k], v[j+1][k+1]).  A
  * trilinear sample then takes two 16-byte loads instead of eight gathers;
  * every tap value is the one pf_g2p_advect reads (sums within rounding).
+ * max_speed (device float, may be NULL): cleared on the stream, then set to
+ * the largest |v| over the FLIP particles (pstate 0) as this pass leaves
+ * them: the value pf_particle_max_speed would return right after the pass
+ * (pfflip/kernels.py:552-564 as called by pfflip/sim.py:157-166), so the next
+ * step's CFL dt needs no separate particle pass.
  * Same arguments and results otherwise. */
 size_t pf_g2p_workspace_bytes(const pf_grid* g);
 int pf_g2p_advect_packed(const pf_grid* g, int64_t n, float* pos4, float* vel4, const float* vel_x,
                          const float* vel_y, const float* vel_z, const float* vstar_x, const float* vstar_y,
                          const float* vstar_z, const float* vliq_x, const float* vliq_y, const float* vliq_z,
                          const int32_t* solid, float alpha_liquid, float alpha_air, float dt, const float lo[3],
-                         const float hi[3], int32_t do_g2p, int32_t do_advect, void* workspace,
+                         const float hi[3], int32_t do_g2p, int32_t do_advect, float* max_speed, void* workspace,
                          size_t workspace_bytes, void* stream);
 
 /* max |v| over particles with pstate == 0, written to the device float *out;

@@ -326,7 +326,7 @@ def test_g2p_packed_matches_unpaired(flags):
         args = [C.byref(g), n, p.data_ptr(), v.data_ptr(), *(t.data_ptr() for t in u), *(t.data_ptr() for t in us),
                 *(t.data_ptr() for t in ul), None, 0.985, 0.96, 0.01, lo, hi, do_g2p, do_adv]
         if packed:
-            N.call("pf_g2p_advect_packed", *args, ws.data_ptr(), ws.numel(), N.stream())
+            N.call("pf_g2p_advect_packed", *args, None, ws.data_ptr(), ws.numel(), N.stream())
         else:
             N.call("pf_g2p_advect", *args, N.stream())
         outs.append((p.cpu().numpy(), v.cpu().numpy()))
@@ -356,3 +356,53 @@ def test_extrapolation_level_passes_equal_tiled_sweeps(sweeps):
     for x, y, k in zip(a, b, kn):
         assert torch.equal(x.view(torch.int32), y.view(torch.int32))
         assert set(torch.unique(k).tolist()) <= {0, 1}
+
+
+def test_particle_max_speed_matches_oracle():
+    """CFL speed (pfflip/kernels.py:552-564): max |v| over FLIP particles only;
+    droplets and dead particles, given far larger speeds here, do not count."""
+    cfg = Config(res=(24, 20, 36), dx=1 / 24, ppc=8, droplets=False)
+    sim = Simulator(cfg)
+    rng = np.random.default_rng(31)
+    n = 150_001
+    L = np.array(cfg.res) * cfg.dx
+    pos = (rng.random((n, 3)) * L).astype(np.float32)
+    vel = rng.standard_normal((n, 3)).astype(np.float32)
+    st = np.zeros(n, np.int32)
+    st[::97] = 1
+    st[5::101] = 2
+    vel[st != 0] *= 100.0
+    sim.set_particles(pos, vel, (rng.random(n) < 0.5).astype(np.int32))
+    sim.pstate.assign(st)
+    N.call("pf_particle_max_speed", sim.n_particles, sim._pos4.data_ptr(), sim._vel4.data_ptr(),
+           sim._scal.data_ptr(), N.stream())
+    got = float(sim._scal[0].item())
+    ref = float(O._fn("particle_max_speed", np.float32)(n, np.ascontiguousarray(vel), st))
+    assert abs(got - ref) <= 1e-6 * ref
+    assert got < 10.0  # the droplets' speeds (~100x) are excluded
+
+
+def test_step_leaves_the_cfl_speed_on_the_device():
+    """The step's last particle pass reduces the FLIP particles' max speed, so
+    dt_from_cfl after a step reads it without a particle pass; it equals the
+    separate reduction over the particles the step left and the oracle's."""
+    cfg = Config(res=(32, 32, 32), dx=1 / 32, ppc=8, seed=42, droplets=False)
+    sim = Simulator(cfg)
+    sim.set_particles(*scenes.dam_break(cfg))
+    assert not sim._vmax_valid
+    for _ in range(3):
+        sim.step(sim.dt_from_cfl())
+    assert sim._vmax_valid
+    launches = N.launch_count()
+    fused = float(sim._scal[2].item())
+    dt_fused = sim.dt_from_cfl()
+    assert N.launch_count() == launches  # no particle pass
+    sim._vmax_valid = False
+    dt_sep = sim.dt_from_cfl()
+    sep = float(sim._scal[0].item())
+    assert abs(fused - sep) <= 1e-6 * sep and abs(dt_fused - dt_sep) <= 1e-6 * dt_sep
+    ref = float(O._fn("particle_max_speed", np.float32)(sim.n_particles, np.ascontiguousarray(sim.pv.numpy()),
+                                                        sim.pstate.numpy()))
+    assert abs(fused - ref) <= 1e-6 * ref
+    sim.pv.assign(sim.pv.numpy() * 2.0)  # any write outside the step invalidates it
+    assert not sim._vmax_valid
