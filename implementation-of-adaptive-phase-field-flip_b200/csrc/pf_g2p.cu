@@ -189,12 +189,6 @@ __global__ void __launch_bounds__(256) k_g2p_advect(const __grid_constant__ G2PA
     V.x = v[0]; V.y = v[1]; V.z = v[2];
     a.pos[p] = P;
     a.vel[p] = V;
-    if (flip) vmax = fmaxf(vmax, sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
-  }
-  if (a.max_speed) {  // uniform: every thread of the grid takes this branch or none does
-    __shared__ float sh[40];
-    vmax = block_max<256>(vmax, sh);
-    if (threadIdx.x == 0) atomic_max_nonneg(a.max_speed, vmax);
   }
 }
 
