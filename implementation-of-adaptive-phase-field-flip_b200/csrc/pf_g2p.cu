@@ -305,7 +305,7 @@ __device__ __forceinline__ void sample_vel_packed(const G2PPackedArgs& a, bool l
 }
 
 __global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(const __grid_constant__ G2PPackedArgs a) {
-  float vmax = 0.f;  // CFL speed of this thread's FLIP particles (pfflip/kernels.py:552-564)
+  float vmax = 0.f;  // CFL speed^2 of this thread's FLIP particles (pfflip/kernels.py:552-564)
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
     float4 P = a.pos[p];
     float4 V = a.vel[p];
@@ -373,11 +373,12 @@ __global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(const __grid_const
     V.x = v[0]; V.y = v[1]; V.z = v[2];
     a.pos[p] = P;
     a.vel[p] = V;
-    if (flip) vmax = fmaxf(vmax, sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+    if (flip) vmax = fmaxf(vmax, v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
   }
   if (a.max_speed) {  // uniform: every thread of the grid takes this branch or none does
     __shared__ float sh[40];
-    vmax = block_max<256>(vmax, sh);
+    // sqrt is correctly rounded and monotone: the root of the max is the max of the roots
+    vmax = sqrtf(block_max<256>(vmax, sh));
     if (threadIdx.x == 0) atomic_max_nonneg(a.max_speed, vmax);
   }
 }
