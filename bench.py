@@ -79,8 +79,11 @@ def parse():
     ap.add_argument("--adjoint-steps", type=int, default=20)
     ap.add_argument("--no-adjoint-fd", action="store_true",
                     help="skip the check of the gradient against FP64 central differences of the CPU oracle")
-    ap.add_argument("--rt", action="store_true",
-                    help="also time the Rayleigh-Taylor workload (256^3, 8 ppc, 16 modes), FP32 and 16-bit hierarchy")
+    ap.add_argument("--no-rt", action="store_true",
+                    help="skip the Rayleigh-Taylor legs (256^3 forward, FP32 and 16-bit hierarchy; 128^3 a_k gradient)")
+    ap.add_argument("--rt-grad-res", type=int, default=128)
+    ap.add_argument("--rt-grad-steps", type=int, default=50)
+    ap.add_argument("--no-rt-fd", action="store_true", help="skip the 32^3 FP64 finite-difference check of the a_k gradient")
     ap.add_argument("--rt-only", action="store_true", help="only the Rayleigh-Taylor leg (prints its JSON)")
     ap.add_argument("--rt-res", type=int, default=256)
     ap.add_argument("--adjoint-fd-res", type=int, default=None,
@@ -431,10 +434,12 @@ def run_ours(args):
         torch.cuda.empty_cache()
         line["adjoint"] = adjoint_leg(args)
 
-    if args.rt and rank == 0:
+    if not args.no_rt and rank == 0:
         sim = None
         torch.cuda.empty_cache()
         line["rayleigh_taylor"] = rt_leg(args)
+        torch.cuda.empty_cache()
+        line["rayleigh_taylor"]["gradient"] = rt_grad_leg(args)
 
     # CPU baseline: the oracle on a bounded sample of the same workload
     if not args.no_cpu_baseline and rank == 0 and world == 1:
@@ -628,6 +633,24 @@ def accuracy_leg(args, pos, vel, pt, dt, warm_steps=2):
     return out
 
 
+def rt_seed_device(cfg, dev, chunk=1 << 23):
+    """Rayleigh-Taylor particles on the device: the jittered lattice tagged by
+    reference height (heavy above Ly/2), displaced vertically by the 16 modes
+    (scenes.rt_profile) chunk by chunk on the GPU."""
+    import torch
+
+    from pfflip import scenes
+
+    pos_ref, ptype, amps, waves = scenes.rayleigh_taylor_lattice(cfg)
+    x = torch.from_numpy(pos_ref).to(dev)
+    a = torch.tensor(amps, dtype=torch.float64, device=dev)
+    for s0 in range(0, x.shape[0], chunk):
+        xs = x[s0:s0 + chunk]
+        d = scenes.rt_profile(xs.double(), waves, cfg.domain_size, xp=torch) @ a
+        xs[:, 1] = (xs[:, 1].double() + d).float()
+    return x, ptype, amps, waves
+
+
 def rt_leg(args):
     """Rayleigh-Taylor: heavy phase (1000) over light (1) across
     y = 0.5 + sum_k a_k cos(2 pi (m_k x + n_k z)), 16 modes with a_k ~ U(0, 0.01)
@@ -635,15 +658,17 @@ def rt_leg(args):
     FP32 step and of the 16-bit-hierarchy step at the same fixed dt."""
     import torch
 
-    from pfflip import Config, Simulator, scenes
+    from pfflip import Config, Simulator
 
     r = args.rt_res
     base = Config(res=(r, r, r), dx=1.0 / r, ppc=8, seed=42, droplets=False, pcg_tol=args.tol, device="cuda")
+    dev = torch.device("cuda")
     t0 = time.perf_counter()
-    pos, vel, pt, amps, waves = scenes.rayleigh_taylor_modes(base)
+    pos, pt, amps, waves = rt_seed_device(base, dev)
     seed_s = time.perf_counter() - t0
+    vel = torch.zeros_like(pos)
     dt = fixed_dt(base.dx)
-    out = {"workload": f"rayleigh_taylor {r}^3 8ppc 16 modes", "particles": int(len(pos)), "dt": dt,
+    out = {"workload": f"rayleigh_taylor {r}^3 8ppc 16 modes", "particles": int(pos.shape[0]), "dt": dt,
            "seed_s": seed_s, "modes": {"a": [float(a) for a in amps], "mn": [[int(m), int(n)] for m, n in waves]}}
     for prec in ("fp32", "fp16"):
         cfg = Config(res=(r, r, r), dx=1.0 / r, ppc=8, seed=42, droplets=False, pcg_tol=args.tol, device="cuda",
@@ -663,6 +688,71 @@ def rt_leg(args):
                      "pcg_iter_mean": float(np.mean([x["pcg_iter"] for x in recs])),
                      "max_div": float(recs[-1]["max_div"])}
         del sim
+        torch.cuda.empty_cache()
+    out["fp16"]["speedup_vs_fp32"] = out["fp32"]["ms_per_step"] / out["fp16"]["ms_per_step"]
+    return out
+
+
+def rt_grad_leg(args):
+    """Gradient of the final interface-height variance of the Rayleigh-Taylor
+    scene with respect to the 16 mode amplitudes (pfflip.adjoint.
+    RTAmplitudeGradient), at --rt-grad-res with --rt-grad-steps steps and
+    checkpoints every 5; checked against FP64 central differences of the
+    oracle at 32^3 / 20 steps on the two largest components."""
+    import torch
+
+    from pfflip import Config
+    from pfflip.adjoint import RTAmplitudeGradient
+
+    def cfg_at(r):
+        return Config(res=(r, r, r), dx=1.0 / r, ppc=8, seed=42, droplets=False, pcg_tol=1e-6, pcg_max_iter=400,
+                      device="cuda")
+
+    r, steps = args.rt_grad_res, args.rt_grad_steps
+    cfg = cfg_at(r)
+    dt = fixed_dt(cfg.dx)
+    g = RTAmplitudeGradient(cfg, dt, steps, checkpoint_every=5, adjoint_tol=1e-6)
+    g.gradient()  # warm-up
+    a = torch.tensor(g.amps0, dtype=torch.float64, device="cuda", requires_grad=True)
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    torch.cuda.synchronize()
+    g.ds.adjoint_solves.clear()
+    e0.record()
+    loss = g.loss(a)
+    e1.record()
+    loss.backward()
+    e2.record()
+    torch.cuda.synchronize()
+    out = {"workload": f"rayleigh_taylor {r}^3 8ppc, {steps} steps from rest, checkpoint every 5; "
+                       "loss = variance over (x, z) columns of dx * sum_y (1 - phi)",
+           "particles": int(g.pos_ref.shape[0]), "dt": dt, "loss": float(loss.detach()),
+           "grad_a": a.grad.cpu().numpy().tolist(), "forward_ms": e0.elapsed_time(e1),
+           "backward_ms": e1.elapsed_time(e2),
+           "adjoint_solve_iters_mean": float(np.mean([it for it, _ in g.ds.adjoint_solves]))}
+    del g
+    torch.cuda.empty_cache()
+    if not args.no_rt_fd:
+        from oracle import oracle as O
+        from pfflip import scenes
+
+        fr, fsteps, eps = 32, 20, 1e-6
+        cf = cfg_at(fr)
+        dtf = fixed_dt(cf.dx)
+        gs = RTAmplitudeGradient(cf, dtf, fsteps, checkpoint_every=5, adjoint_tol=1e-6)
+        _, grad = gs.gradient()
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        comps = []
+        for k in np.argsort(-np.abs(grad))[:2]:
+            lp, lm = (O.rt_interface_variance(
+                cf, scenes.rt_displace(gs.pos_ref_host, gs.amps0 + sg * eps * np.eye(16)[k], gs.waves,
+                                       cf.domain_size), gs.ptype, dtf, fsteps, nthreads=threads) for sg in (1.0, -1.0))
+            fd = (lp - lm) / (2 * eps)
+            comps.append({"k": int(k), "grad": float(grad[k]), "fd": fd, "rel_err": abs(grad[k] - fd) / abs(fd)})
+        out["fd_check"] = {"res": fr, "steps": fsteps, "eps": eps, "oracle": "binary64, solve to 1e-12",
+                           "components": comps, "max_rel_err": max(c["rel_err"] for c in comps),
+                           "cpu_s": time.perf_counter() - t0, "threads": threads}
+        del gs
         torch.cuda.empty_cache()
     return out
 
@@ -771,7 +861,9 @@ def main():
         import torch
 
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        print(json.dumps({"rayleigh_taylor": rt_leg(args)}), flush=True)
+        rt = rt_leg(args)
+        rt["gradient"] = rt_grad_leg(args)
+        print(json.dumps({"rayleigh_taylor": rt}), flush=True)
         return 0
     if args.adjoint_only:
         import torch

@@ -248,3 +248,58 @@ class _Phase(torch.autograd.Function):
         with torch.no_grad():
             gx = ctx.dsim._phase_backward(x, gphi.contiguous())
         return gx, None
+
+
+class RTAmplitudeGradient:
+    """Gradient of the final interface-height variance of the Rayleigh-Taylor
+    scene with respect to its 16 mode amplitudes a_k.
+
+    The liquid (heavy, rho_l) tags are piecewise constant in a_k, so the
+    amplitudes enter through the particle positions instead: the jittered
+    lattice is tagged by its reference height (heavy above Ly/2) and displaced
+    vertically by D a, D[p, k] = Ly sin^2(pi y/Ly) cos(2 pi (m_k x + n_k z))
+    (scenes.rt_profile), which carries the plane Ly/2 onto the interface
+    0.5 + sum_k a_k cos(...).  After ``steps`` steps the light-phase height of
+    every (x, z) column is h = dx sum_y (1 - phi) and the loss is the variance
+    of h over the columns.  d loss / d a = D^T (d loss / d x0) through the
+    adjoint rollout (DiffSim) and the adjoint of eq. (7)."""
+
+    def __init__(self, cfg: Config, dt: float, steps: int, checkpoint_every: int = 5,
+                 adjoint_tol: float | None = 1e-6, n_modes: int = 16):
+        from . import scenes
+
+        pos_ref, ptype, amps, waves = scenes.rayleigh_taylor_lattice(cfg, n_modes)
+        self.cfg = cfg
+        self.steps = int(steps)
+        self.amps0 = np.asarray(amps, np.float64)
+        self.waves = np.asarray(waves)
+        self.pos_ref_host = pos_ref
+        self.ptype = ptype
+        self.ds = DiffSim(cfg, ptype, dt, checkpoint_every=checkpoint_every, adjoint_tol=adjoint_tol)
+        dev = self.ds.sim.dev
+        ref = torch.from_numpy(pos_ref).to(dev)
+        self.pos_ref = ref
+        self.profile = scenes.rt_profile(ref.double(), self.waves, cfg.domain_size, xp=torch).float()
+
+    def positions(self, a):
+        """Initial positions for amplitudes a ((n_modes,) tensor)."""
+        dy = self.profile @ a.to(device=self.profile.device, dtype=torch.float32)
+        x = self.pos_ref
+        return torch.stack((x[:, 0], x[:, 1] + dy, x[:, 2]), dim=1)
+
+    def interface_variance(self, phi):
+        h = (1.0 - phi.double()).sum(dim=1) * self.cfg.dx  # (nx, nz) light-phase column heights
+        return ((h - h.mean()) ** 2).mean()
+
+    def loss(self, a):
+        x0 = self.positions(a)
+        xT, _ = self.ds.rollout(x0, torch.zeros_like(x0), self.steps)
+        return self.interface_variance(self.ds.phase_field(xT))
+
+    def gradient(self, a=None):
+        """(loss, d loss / d a) at amplitudes a (default: the seeded ones)."""
+        a = torch.tensor(self.amps0 if a is None else a, dtype=torch.float64, device=self.ds.sim.dev,
+                         requires_grad=True)
+        loss = self.loss(a)
+        loss.backward()
+        return float(loss.detach()), a.grad.double().cpu().numpy()

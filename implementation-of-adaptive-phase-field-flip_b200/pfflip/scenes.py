@@ -256,3 +256,44 @@ def solve_problem(res=(128, 128, 128), seed: int = 42, rho_l=1000.0, density_rat
     b = rng.standard_normal(res)
     b -= b.mean()
     return out[0], out[1], out[2], b.astype(np.float32), phi.astype(np.float32)
+
+
+def rayleigh_taylor_lattice(cfg: Config, n_modes: int = 16):
+    """The Rayleigh-Taylor scene in a form that is differentiable in the mode
+    amplitudes: the jittered lattice of ``seed`` with the heavy phase (liquid
+    tag) where the *reference* height y_ref > 0.5 Ly, to be displaced by
+    ``rt_displace``.  The tags do not depend on a_k; the positions do,
+    smoothly.  Returns (pos_ref, ptype, amps, waves)."""
+    amps, waves = rt_modes(cfg.seed, n_modes)
+    sy = cfg.domain_size[1]
+    pos, _, ptype = seed(cfg, lambda p: p[:, 1] > 0.5 * sy)
+    return pos, ptype, amps, waves
+
+
+def rt_profile(pos, waves, domain, xp=np):
+    """Per particle and mode: the vertical displacement a unit amplitude of
+    mode k gives the particle at reference position pos,
+        D[p, k] = Ly sin^2(pi y/Ly) cos(2 pi (m_k x/Lx + n_k z/Lz)).
+    sin^2 is 1 at y = Ly/2 and 0 at the floor and the lid, so
+    y -> y + D a maps the plane y_ref = Ly/2 onto 0.5 + sum_k a_k cos(...) (in
+    unit-box coordinates), keeps particles inside the box, and is monotone in y
+    while pi |sum_k a_k cos(...)| < 1 (always for a_k <= 0.01 and 16 modes).
+    ``xp`` is numpy (float64 host) or torch (device tensors)."""
+    sx, sy, sz = domain
+    x, y, z = pos[:, 0:1], pos[:, 1:2], pos[:, 2:3]
+    if xp is np:
+        w = np.asarray(waves, np.float64)
+        m, n = w[None, :, 0], w[None, :, 1]
+    else:
+        w = xp.as_tensor(np.asarray(waves), dtype=pos.dtype, device=pos.device)
+        m, n = w[None, :, 0], w[None, :, 1]
+    return sy * xp.sin(np.pi * y / sy) ** 2 * xp.cos(2 * np.pi * (m * x / sx + n * z / sz))
+
+
+def rt_displace(pos_ref, amps, waves, domain):
+    """Positions of the Rayleigh-Taylor lattice for amplitudes ``amps`` (host,
+    float64 arithmetic; float32 result)."""
+    p = np.asarray(pos_ref, np.float64)
+    out = p.copy()
+    out[:, 1] += rt_profile(p, waves, domain) @ np.asarray(amps, np.float64)
+    return out

@@ -475,3 +475,20 @@ class OracleSim:
                "max_div": div, "droplets": int((self.pstate == 1).sum()) if self.cfg.droplets else 0}
         self.stats.append(rec)
         return rec
+
+
+def rt_interface_variance(cfg, pos, ptype, dt, steps, nthreads=1):
+    """The Rayleigh-Taylor gradient's loss on the binary64 oracle (solve to
+    1e-12): run ``steps`` steps from rest at ``pos``, then the variance over
+    the (x, z) columns of the light-phase height h = dx sum_y (1 - phi)."""
+    import dataclasses
+
+    c64 = dataclasses.replace(cfg, pcg_tol=1e-12, pcg_max_iter=1000)
+    sim = OracleSim(c64, dtype=np.float64, nthreads=nthreads, stencil="flux")
+    sim.set_particles(np.asarray(pos, np.float64), np.zeros((len(pos), 3)), ptype)
+    for _ in range(steps):
+        sim.step(dt)
+    sim._p2g()
+    sim._phase_field_and_coefficients()
+    h = (1.0 - sim.phi_cell).sum(axis=1) * cfg.dx
+    return float(((h - h.mean()) ** 2).mean())
