@@ -197,10 +197,10 @@ __global__ void __launch_bounds__(256) k_g2p_advect(const __grid_constant__ G2PA
 // f = (i, j, k) of a face grid, q[f] = (v[j][k], v[j][k+1], v[j+1][k],
 // v[j+1][k+1]) of the same i-plane, with j+1 -> j and k+1 -> k on the last
 // plane of the grid.  A trilinear sample is then two 16-byte loads (the lower
-// and the upper i-plane) instead of eight gathers.  Where the frame clamps
-// the j or k taps to one index (lo == hi) the upper taps take the lower
-// values, so every tap value is the one the unpaired kernel reads.  u, u* and
-// the extrapolated field ul each get their quads.
+// and the upper i-plane) instead of eight gathers.  Interpolation runs as
+// lerp chains (t (b - a) + a) over the quads; the reference's weighted sum of
+// the eight taps rounds differently, within an ulp or two.  u, u* and the
+// extrapolated field ul each get their quads.
 struct FacePack {
   FaceSpace s;
   const float* u[3];
@@ -239,73 +239,109 @@ __global__ void __launch_bounds__(C3_NT) k_pack_faces(FacePack fp) {
   if (const float* ul = fp.ul[ax]) fp.ql[ax][f] = make_float4(ul[f], ul[f + dk], ul[f + dj], ul[f + dj + dk]);
 }
 
-// the two i-planes of face grid c for a frame, and the (j, k) weights
-struct Rows {
-  int row[2];
-  float wi[2];
-  float wj0, wj1, wk0, wk1;
-  bool cj, ck;  // j / k taps clamped to one index
+// Per position, the lower tap index and the upper weight of each axis d for
+// node offset 0 (v = 0: the normal axis of face grid d, extent n_d + 1) and
+// 0.5 (v = 1: extent n_d), as pfflip/kernels.py:52-79 computes them:
+//   g = x/dx - o, i0 = floor(g), t = g - i0, taps clamp(i0) and clamp(i0 + 1).
+// The offset-0.5 frame follows from the offset-0 one: with q = x/dx,
+// i = floor(q) and s = q - i, floor(q - 0.5) is i (s >= 0.5) or i - 1 and
+// t = s - 0.5 or s + 0.5, the binary32 values the reference computes wherever
+// its two taps differ (q - 0.5 is exact for q >= 0.5; below, both taps clamp
+// to index 0).  The index clamps are folded into the weight: both taps at 0
+// is taps (0, 1) with t = 0, both at the last index is (last - 1, last) with
+// t = 1, so the upper tap is always lo + 1; frames away from the walls skip
+// the clamps.
+struct LeanFrame {
+  int lo[3][2];
+  float t[3][2];
 };
 
-__device__ __forceinline__ void rows_of(const Frame& fr, int c, int ny, int nz, Rows& r) {
-  const int vi = c == 0 ? 0 : 1, vj = c == 1 ? 0 : 1, vk = c == 2 ? 0 : 1;
-  const int n1 = ny + (c == 1), n2 = nz + (c == 2);
-  const float tx = fr.t[0][vi], ty = fr.t[1][vj], tz = fr.t[2][vk];
-  const int jk = fr.lo[1][vj] * n2 + fr.lo[2][vk];
-  r.row[0] = fr.lo[0][vi] * n1 * n2 + jk;
-  r.row[1] = fr.hi[0][vi] * n1 * n2 + jk;
-  r.wi[0] = 1.f - tx;
-  r.wi[1] = tx;
-  r.wj0 = 1.f - ty;
-  r.wj1 = ty;
-  r.wk0 = 1.f - tz;
-  r.wk1 = tz;
-  r.cj = fr.lo[1][vj] == fr.hi[1][vj];
-  r.ck = fr.lo[2][vk] == fr.hi[2][vk];
-}
-
-// the four taps of a quad after the frame's clamps: (j, k), (j, k+1), (j+1, k), (j+1, k+1)
-__device__ __forceinline__ float4 taps(float4 v, const Rows& r) {
-  const float b = r.ck ? v.x : v.y;
-  const float d = r.ck ? v.z : v.w;
-  return r.cj ? make_float4(v.x, b, v.x, b) : make_float4(v.x, b, v.z, d);
-}
-
-__device__ __forceinline__ float bilerp(float4 t, const Rows& r) {
-  return r.wj0 * (r.wk0 * t.x + r.wk1 * t.y) + r.wj1 * (r.wk0 * t.z + r.wk1 * t.w);
-}
-
-// G2P sample of component c: delta = I(u - u*) tap by tap, pic = I(u)
-__device__ __forceinline__ void sample_g2p_packed(const float4* __restrict__ qu, const float4* __restrict__ qs,
-                                                  const Rows& r, float& delta, float& pic) {
-  float ad = 0.f, ap = 0.f;
+__device__ __forceinline__ void lean_frame(const float x[3], float inv_dx, const int n[3], LeanFrame& f) {
+  bool edge = false;
 #pragma unroll
-  for (int q = 0; q < 2; ++q) {
-    const float4 u = taps(__ldg(qu + r.row[q]), r), w = taps(__ldg(qs + r.row[q]), r);
-    ad += r.wi[q] * bilerp(make_float4(u.x - w.x, u.y - w.y, u.z - w.z, u.w - w.w), r);
-    ap += r.wi[q] * bilerp(u, r);
+  for (int d = 0; d < 3; ++d) {
+    const float q = x[d] * inv_dx;
+    const float fl = floorf(q);
+    const int i = (int)fl;
+    const float s = q - fl;
+    const bool up = s >= 0.5f;
+    f.lo[d][0] = i;
+    f.t[d][0] = s;
+    f.lo[d][1] = up ? i : i - 1;
+    f.t[d][1] = s + (up ? -0.5f : 0.5f);
+    edge = edge || i < 1 || i > n[d] - 2;
   }
-  delta = ad;
-  pic = ap;
-}
-
-__device__ __forceinline__ float sample_quad(const float4* __restrict__ q, const Rows& r) {
-  return r.wi[0] * bilerp(taps(__ldg(q + r.row[0]), r), r) + r.wi[1] * bilerp(taps(__ldg(q + r.row[1]), r), r);
-}
-
-// RK3 sample: liquid particles read the extrapolated field, air the raw one
-__device__ __forceinline__ void sample_vel_packed(const G2PPackedArgs& a, bool liquid, const Frame& fr,
-                                                  float out[3]) {
+  if (edge) {
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    Rows r;
-    rows_of(fr, c, a.ny, a.nz, r);
-    out[c] = sample_quad(liquid ? a.ql[c] : a.qu[c], r);
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        const int last = v == 0 ? n[d] : n[d] - 1;
+        if (f.lo[d][v] < 0) {
+          f.lo[d][v] = 0;
+          f.t[d][v] = 0.f;
+        } else if (f.lo[d][v] >= last) {
+          f.lo[d][v] = last - 1;
+          f.t[d][v] = 1.f;
+        }
+      }
   }
+}
+
+__device__ __forceinline__ float lerpf(float a, float b, float t) { return fmaf(t, b - a, a); }
+
+// bilinear in (j, k) of one quad (v[j][k], v[j][k+1], v[j+1][k], v[j+1][k+1])
+__device__ __forceinline__ float bilerp_q(float4 v, float tj, float tk) {
+  return lerpf(lerpf(v.x, v.y, tk), lerpf(v.z, v.w, tk), tj);
+}
+
+// face grid C: node offsets of the three axes (0 on the normal axis), the
+// quad index of the frame's lower (i, j, k) taps, and the upper-plane stride
+template <int C> struct Comp {
+  static constexpr int VI = C == 0 ? 0 : 1, VJ = C == 1 ? 0 : 1, VK = C == 2 ? 0 : 1;
+};
+
+template <int C>
+__device__ __forceinline__ int quad_row(const LeanFrame& f, int n1, int n2) {
+  return (f.lo[0][Comp<C>::VI] * n1 + f.lo[1][Comp<C>::VJ]) * n2 + f.lo[2][Comp<C>::VK];
+}
+
+template <int C>
+__device__ __forceinline__ float sample_quad(const float4* __restrict__ q, const LeanFrame& f, int n1, int n2) {
+  const int row = quad_row<C>(f, n1, n2);
+  const float4 v0 = __ldg(q + row), v1 = __ldg(q + row + n1 * n2);
+  const float tj = f.t[1][Comp<C>::VJ], tk = f.t[2][Comp<C>::VK];
+  return lerpf(bilerp_q(v0, tj, tk), bilerp_q(v1, tj, tk), f.t[0][Comp<C>::VI]);
+}
+
+// G2P sample of component C: delta = I(u - u*) tap by tap, pic = I(u)
+template <int C>
+__device__ __forceinline__ void sample_g2p_lean(const float4* __restrict__ qu, const float4* __restrict__ qs,
+                                                const LeanFrame& f, int n1, int n2, float& delta, float& pic) {
+  const int row = quad_row<C>(f, n1, n2);
+  const int up = n1 * n2;
+  const float4 u0 = __ldg(qu + row), u1 = __ldg(qu + row + up);
+  const float4 s0 = __ldg(qs + row), s1 = __ldg(qs + row + up);
+  const float tj = f.t[1][Comp<C>::VJ], tk = f.t[2][Comp<C>::VK], ti = f.t[0][Comp<C>::VI];
+  pic = lerpf(bilerp_q(u0, tj, tk), bilerp_q(u1, tj, tk), ti);
+  const float4 d0 = make_float4(u0.x - s0.x, u0.y - s0.y, u0.z - s0.z, u0.w - s0.w);
+  const float4 d1 = make_float4(u1.x - s1.x, u1.y - s1.y, u1.z - s1.z, u1.w - s1.w);
+  delta = lerpf(bilerp_q(d0, tj, tk), bilerp_q(d1, tj, tk), ti);
+}
+
+// RK3 sample of the velocity: liquid particles read the extrapolated field,
+// air the raw one
+__device__ __forceinline__ void sample_vel_lean(const G2PPackedArgs& a, bool liquid, const LeanFrame& f,
+                                                float out[3]) {
+  const int ny = a.ny, nz = a.nz;
+  out[0] = sample_quad<0>(liquid ? a.ql[0] : a.qu[0], f, ny, nz);
+  out[1] = sample_quad<1>(liquid ? a.ql[1] : a.qu[1], f, ny + 1, nz);
+  out[2] = sample_quad<2>(liquid ? a.ql[2] : a.qu[2], f, ny, nz + 1);
 }
 
 __global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(const __grid_constant__ G2PPackedArgs a) {
   float vmax = 0.f;  // CFL speed^2 of this thread's FLIP particles (pfflip/kernels.py:552-564)
+  const int nn[3] = {a.nx, a.ny, a.nz};
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
     float4 P = a.pos[p];
     float4 V = a.vel[p];
@@ -315,19 +351,17 @@ __global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(const __grid_const
     float x[3] = {P.x, P.y, P.z};
     float v[3] = {V.x, V.y, V.z};
     const bool flip = pstate == 0;
-    Frame fx;
-    if (flip && (a.do_g2p || a.do_advect)) make_frame(x, a.inv_dx, a.nx, a.ny, a.nz, fx);
+    LeanFrame fx;
+    if (flip && (a.do_g2p || a.do_advect)) lean_frame(x, a.inv_dx, nn, fx);
     float pic[3];  // I(u) at x: an air particle's first RK3 stage samples the same field there
     if (a.do_g2p && flip) {
       const float alpha = liquid ? a.a_liq : a.a_air;
+      float delta[3];
+      sample_g2p_lean<0>(a.qu[0], a.qs[0], fx, a.ny, a.nz, delta[0], pic[0]);
+      sample_g2p_lean<1>(a.qu[1], a.qs[1], fx, a.ny + 1, a.nz, delta[1], pic[1]);
+      sample_g2p_lean<2>(a.qu[2], a.qs[2], fx, a.ny, a.nz + 1, delta[2], pic[2]);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        Rows r;
-        rows_of(fx, c, a.ny, a.nz, r);
-        float delta;
-        sample_g2p_packed(a.qu[c], a.qs[c], r, delta, pic[c]);
-        v[c] = alpha * (v[c] + delta) + (1.f - alpha) * pic[c];
-      }
+      for (int c = 0; c < 3; ++c) v[c] = alpha * (v[c] + delta[c]) + (1.f - alpha) * pic[c];
     }
     if (a.do_advect) {
       if (flip) {
@@ -336,18 +370,18 @@ __global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(const __grid_const
 #pragma unroll
           for (int c = 0; c < 3; ++c) k1[c] = pic[c];
         } else {
-          sample_vel_packed(a, liquid, fx, k1);
+          sample_vel_lean(a, liquid, fx, k1);
         }
         const float h1 = 0.5f * a.dt, h2 = 0.75f * a.dt;
 #pragma unroll
         for (int c = 0; c < 3; ++c) y[c] = x[c] + h1 * k1[c];
-        Frame fy;
-        make_frame(y, a.inv_dx, a.nx, a.ny, a.nz, fy);
-        sample_vel_packed(a, liquid, fy, k2);
+        LeanFrame fy;
+        lean_frame(y, a.inv_dx, nn, fy);
+        sample_vel_lean(a, liquid, fy, k2);
 #pragma unroll
         for (int c = 0; c < 3; ++c) y[c] = x[c] + h2 * k2[c];
-        make_frame(y, a.inv_dx, a.nx, a.ny, a.nz, fy);
-        sample_vel_packed(a, liquid, fy, k3);
+        lean_frame(y, a.inv_dx, nn, fy);
+        sample_vel_lean(a, liquid, fy, k3);
         const float c1 = 2.0f / 9.0f, c2 = 3.0f / 9.0f, c3 = 4.0f / 9.0f;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -455,6 +489,7 @@ extern "C" int pf_g2p_advect_packed(const pf_grid* g, int64_t n, float* pos4, fl
                                     void* workspace, size_t workspace_bytes, void* stream) {
   PF_REQUIRE(g && pos4 && vel4 && vel_x && vel_y && vel_z, "null argument");
   PF_REQUIRE(g->nx > 0 && g->ny > 0 && g->nz > 0, "bad grid");
+  PF_REQUIRE(g->nx >= 2 && g->ny >= 2 && g->nz >= 2, "the quad pass needs at least 2 cells per axis");
   PF_REQUIRE(!do_g2p || (vstar_x && vstar_y && vstar_z), "u* fields required for G2P");
   PF_REQUIRE(!do_advect || (vliq_x && vliq_y && vliq_z && lo && hi), "extrapolated fields and bounds required");
   PF_REQUIRE(aligned16(pos4) && aligned16(vel4), "particle streams must be 16-byte aligned");

@@ -13,8 +13,13 @@
 // instead of 64 per particle, and no two lanes of a warp ever add to the same
 // node.  Each tile node is flushed to global memory once (red.global.add).
 //
-// Weights: w = max(1 - d^2/r^2, 0)^3 with d^2 = (fx^2 + fy^2) + fz^2 and
-// fx = (n + o)*dx - x in the reference's order (d^2/r^2 as d^2*(1/r^2)).  The
+// Weights: w = max(1 - d^2/r^2, 0)^3, evaluated in the cell's own scaled
+// frame: per axis xl = x - i*dx (one rounding, the product exact inside the
+// fma), X = xl/r, and for a node at (i + L + o)*dx the scaled offset
+// f = (L + o)*(dx/r) - X; then s = (fx^2 - 1) + fy^2 + fz^2 = d^2/r^2 - 1 and
+// w = -min(s, 0)^3, the sign folded into the particle's mass.  This is the
+// reference's weight to rounding (its d^2 sums in world units; the scaled
+// offsets here carry no more error than its fx = (n + o)*dx - x).  The
 // register box includes nodes outside the reference's window
 // floor(c - R) + 1 .. floor(c + R); those lie at least r away, so their
 // weight is exactly 0, and nodes outside the grid are never flushed.  The
@@ -33,7 +38,7 @@ constexpr size_t PG_SMEM = sizeof(float) * PG_NACC * PG_BOX;
 
 struct P2GArgs {
   int nx, ny, nz;
-  float dx, inv_r2;
+  float dx, inv_r, s_node;  // s_node = dx / r
   float rho_l, rho_g;
   const float4* pos;
   const float4* vel;
@@ -85,43 +90,47 @@ template <int G> struct Box {
     return (PA == 0 ? a : PA == 1 ? b : c) == 0 ? f2_x(v) : f2_y(v);
   }
 
-  __device__ __forceinline__ void node2(f2 s2, f2 ninv, f2 one, f2 mp2, f2 up2, f2& m, f2& q) {
-    const f2 t = f2_relu(f2_fma(s2, ninv, one));
-    const f2 w = f2_mul(f2_mul(t, t), t);
-    const f2 wm = f2_mul(w, mp2);
-    m = f2_add(m, wm);
-    q = (G < 3) ? f2_fma(wm, up2, q) : f2_add(q, w);
+  // one node pair: s = d^2/r^2 - 1 per half; u = min(s, 0), w = -u^3; the
+  // accumulators take m += w m_p and q += w m_p u_G (faces) or q += w (cells)
+  // as fma(u^3, -m_p, m) and fma(u^3, -m_p u_G, q) / fma(u^3, -1, q)
+  __device__ __forceinline__ static void node2(f2 s, f2 nmp2, f2 nq2, f2& m, f2& q) {
+    float a, b;
+    f2_split(s, a, b);
+    const f2 u = f2_make(fminf(a, 0.f), fminf(b, 0.f));
+    const f2 u3 = f2_mul(f2_mul(u, u), u);
+    m = f2_fma(u3, nmp2, m);
+    q = f2_fma(u3, nq2, q);
   }
 
-  // squared distances along one axis to the nodes c + L + o: a pair (o = 0, 1)
-  // for the paired axis, broadcast pairs per node otherwise
-  template <int N, int L, bool PAIRED>
-  __device__ __forceinline__ static void dist2(int c, float off, float x, f2 dx2, f2* out) {
-    const f2 gx = f2_bcast(-x);
+  // scaled squared offsets along one axis to the nodes L + o (o = 0 .. N-1) of
+  // the cell, minus one when M1: a pair (o = 0, 1) for the paired axis,
+  // broadcast pairs per node otherwise.  X = (x - i dx)/r; off = node offset
+  // within its cell (0 or 0.5); sn = dx/r.
+  template <int N, int L, bool PAIRED, bool M1>
+  __device__ __forceinline__ static void dist2(float off, float X, float sn, f2* out) {
+    const f2 nx = f2_bcast(-X), one = f2_bcast(M1 ? -1.f : 0.f);
     if (PAIRED) {
-      const f2 f = f2_fma(f2_make((float)(c + L) + off, (float)(c + L + 1) + off), dx2, gx);
-      out[0] = f2_mul(f, f);
+      const f2 f = f2_fma(f2_make((float)L + off, (float)(L + 1) + off), f2_bcast(sn), nx);
+      out[0] = f2_fma(f, f, one);
     } else {
 #pragma unroll
       for (int o = 0; o < N; ++o) {
-        const f2 f = f2_fma(f2_bcast((float)(c + L + o) + off), dx2, gx);
-        out[o] = f2_mul(f, f);
+        const f2 f = f2_fma(f2_bcast((float)(L + o) + off), f2_bcast(sn), nx);
+        out[o] = f2_fma(f, f, one);
       }
     }
   }
 
-  // add one particle (x, mass, velocity component) of cell (ci, cj, ck)
-  __device__ __forceinline__ void add(int ci, int cj, int ck, const float x[3], float mp, float up, float dx,
-                                      float inv_r2) {
-    const f2 dx2 = f2_bcast(dx), ninv = f2_bcast(-inv_r2), one = f2_bcast(1.f);
-    const f2 mp2 = f2_bcast(mp), up2 = f2_bcast(up);
+  // add one particle (scaled cell-local position X, mass, velocity component)
+  __device__ __forceinline__ void add(const float X[3], float mp, float up, float sn) {
+    const f2 nmp2 = f2_bcast(-mp), nq2 = f2_bcast(G < 3 ? -mp * up : -1.f);
     f2 DX[PA == 0 ? 1 : NX], DY[PA == 1 ? 1 : NY], DZ[PA == 2 ? 1 : NZ];
-    dist2<NX, LX, PA == 0>(ci, OX, x[0], dx2, DX);
-    dist2<NY, LY, PA == 1>(cj, OY, x[1], dx2, DY);
-    dist2<NZ, LZ, PA == 2>(ck, OZ, x[2], dx2, DZ);
+    dist2<NX, LX, PA == 0, true>(OX, X[0], sn, DX);
+    dist2<NY, LY, PA == 1, false>(OY, X[1], sn, DY);
+    dist2<NZ, LZ, PA == 2, false>(OZ, X[2], sn, DZ);
     float dz2 = 0.f;  // cell grid: z node 2
     if (G == 3) {
-      const float f = fmaf((float)(ck + LZ + 2) + OZ, dx, -x[2]);
+      const float f = fmaf((float)(LZ + 2) + OZ, sn, -X[2]);
       dz2 = f * f;
     }
     if (PA == 0) {
@@ -129,14 +138,14 @@ template <int G> struct Box {
       for (int b = 0; b < NY; ++b) {
         const f2 dxy = f2_add(DX[0], DY[b]);
 #pragma unroll
-        for (int c = 0; c < NZ; ++c) node2(f2_add(dxy, DZ[c]), ninv, one, mp2, up2, m2[0][b][c], q2[0][b][c]);
+        for (int c = 0; c < NZ; ++c) node2(f2_add(dxy, DZ[c]), nmp2, nq2, m2[0][b][c], q2[0][b][c]);
       }
     } else if (PA == 1) {
 #pragma unroll
       for (int a = 0; a < NX; ++a) {
         const f2 dxy = f2_add(DX[a], DY[0]);
 #pragma unroll
-        for (int c = 0; c < NZ; ++c) node2(f2_add(dxy, DZ[c]), ninv, one, mp2, up2, m2[a][0][c], q2[a][0][c]);
+        for (int c = 0; c < NZ; ++c) node2(f2_add(dxy, DZ[c]), nmp2, nq2, m2[a][0][c], q2[a][0][c]);
       }
     } else {
 #pragma unroll
@@ -144,13 +153,12 @@ template <int G> struct Box {
 #pragma unroll
         for (int b = 0; b < NY; ++b) {
           const f2 dxy = f2_add(DX[a], DY[b]);
-          node2(f2_add(dxy, DZ[0]), ninv, one, mp2, up2, m2[a][b][0], q2[a][b][0]);
+          node2(f2_add(dxy, DZ[0]), nmp2, nq2, m2[a][b][0], q2[a][b][0]);
           if (G == 3) {
-            const float t = fmaxf(fmaf(f2_x(dxy) + dz2, -inv_r2, 1.f), 0.f);
-            const float w = t * t * t;
-            const float wm = w * mp;
-            m1[a < SX ? a : 0][b < SX ? b : 0] += wm;
-            q1[a < SX ? a : 0][b < SX ? b : 0] += w;
+            const float u = fminf(f2_x(dxy) + dz2, 0.f);
+            const float u3 = u * u * u;
+            m1[a < SX ? a : 0][b < SX ? b : 0] = fmaf(u3, -mp, m1[a < SX ? a : 0][b < SX ? b : 0]);
+            q1[a < SX ? a : 0][b < SX ? b : 0] -= u3;
           }
         }
     }
@@ -206,6 +214,7 @@ __device__ __forceinline__ void p2g_grid(const P2GArgs& a, float* acc, int i, in
                                          int lj, int lane) {
   Box<G> box;
   box.zero();
+  const float ci = (float)i, cj = (float)j, ck = (float)k;
   // one particle of prefetch: the loads of t+1 are in flight while t is splatted
   float4 Pn = make_float4(0.f, 0.f, 0.f, 0.f), Vn = Pn;
   if (s < e) {
@@ -222,8 +231,9 @@ __device__ __forceinline__ void p2g_grid(const P2GArgs& a, float* acc, int i, in
     if ((flags >> PF_PSTATE_SHIFT) & 3) continue;  // droplets / dead particles do not splat
     const float mp = (flags & PF_FLAG_LIQUID) ? a.rho_l : a.rho_g;
     const float up = G == 0 ? V.x : G == 1 ? V.y : V.z;
-    const float x[3] = {P.x, P.y, P.z};
-    box.add(i, j, k, x, mp, up, a.dx, a.inv_r2);
+    const float X[3] = {fmaf(ci, -a.dx, P.x) * a.inv_r, fmaf(cj, -a.dx, P.y) * a.inv_r,
+                        fmaf(ck, -a.dx, P.z) * a.inv_r};
+    box.add(X, mp, up, a.s_node);
   }
   const int a1 = (G < 3) ? G : 6, a2 = (G < 3) ? 3 + G : 7;
   box.flush(acc + a1 * PG_BOX, acc + a2 * PG_BOX, li, lj, lane);
@@ -300,7 +310,8 @@ extern "C" int pf_p2g(const pf_grid* g, int64_t n, const float* pos4, const floa
   P2GArgs a;
   a.nx = nx; a.ny = ny; a.nz = nz;
   a.dx = g->dx;
-  a.inv_r2 = 1.f / (r_p * r_p);
+  a.inv_r = 1.f / r_p;
+  a.s_node = g->dx / r_p;
   a.rho_l = rho_l; a.rho_g = rho_g;
   a.pos = reinterpret_cast<const float4*>(pos4);
   a.vel = reinterpret_cast<const float4*>(vel4);

@@ -492,3 +492,18 @@ def rt_interface_variance(cfg, pos, ptype, dt, steps, nthreads=1):
     sim._phase_field_and_coefficients()
     h = (1.0 - sim.phi_cell).sum(axis=1) * cfg.dx
     return float(((h - h.mean()) ** 2).mean())
+
+
+def stable_central_difference(loss, eps_list=(1e-5, 3e-6, 1e-6, 3e-7), rtol=2e-4):
+    """Central difference (loss(+e) - loss(-e)) / 2e of a scalar function of one
+    step size e, taken away from the function's jumps and kinks: the first two
+    consecutive step sizes of ``eps_list`` whose differences agree to ``rtol``
+    give the value (the smaller step's).  Returns (value, eps, all differences)
+    or (None, None, all differences) when no two agree, i.e. a jump of the
+    loss lies within the largest step of the point."""
+    fds = []
+    for e in eps_list:
+        fds.append((loss(e) - loss(-e)) / (2.0 * e))
+        if len(fds) >= 2 and abs(fds[-1] - fds[-2]) <= rtol * max(abs(fds[-1]), 1e-300):
+            return fds[-1], e, fds
+    return None, None, fds

@@ -211,8 +211,12 @@ def test_unsort_inverts_the_sort_gather():
 def test_rt_amplitude_gradient_matches_fp64_finite_differences():
     """Gradient of the final interface-height variance of the Rayleigh-Taylor
     scene (16 modes) with respect to the mode amplitudes, 32^3 / 8 ppc, 20
-    steps, checkpoints every 5: the two largest components against FP64
-    central differences of the oracle (the same displaced lattice)."""
+    steps, checkpoints every 5, against FP64 central differences of the oracle
+    (the same displaced lattice).  The loss has small jumps: as particles move,
+    liquid tags, valid-face tests and extrapolation masks flip, which the
+    adjoint holds fixed.  A difference is therefore taken only where two
+    consecutive step sizes agree (oracle.stable_central_difference); two
+    components of the largest four must be checked that way."""
     from pfflip.adjoint import RTAmplitudeGradient
 
     cfg = small_cfg(res=32, ppc=8, seed=42)
@@ -220,13 +224,20 @@ def test_rt_amplitude_gradient_matches_fp64_finite_differences():
     steps = 20
     g = RTAmplitudeGradient(cfg, dt, steps, checkpoint_every=5, adjoint_tol=1e-6)
     loss, grad = g.gradient()
-    l64 = O.rt_interface_variance(cfg, scenes.rt_displace(g.pos_ref_host, g.amps0, g.waves, cfg.domain_size),
-                                  g.ptype, dt, steps, nthreads=NTHR)
+
+    def oracle_loss(amps):
+        pos = scenes.rt_displace(g.pos_ref_host, amps, g.waves, cfg.domain_size)
+        return O.rt_interface_variance(cfg, pos, g.ptype, dt, steps, nthreads=NTHR)
+
+    l64 = oracle_loss(g.amps0)
     assert abs(loss - l64) <= 1e-3 * l64, (loss, l64)
-    eps = 1e-6
-    for k in np.argsort(-np.abs(grad))[:2]:
-        lp, lm = (O.rt_interface_variance(
-            cfg, scenes.rt_displace(g.pos_ref_host, g.amps0 + s * eps * np.eye(16)[k], g.waves, cfg.domain_size),
-            g.ptype, dt, steps, nthreads=NTHR) for s in (1.0, -1.0))
-        fd = (lp - lm) / (2 * eps)
-        assert abs(grad[k] - fd) <= 1e-3 * abs(fd), (k, grad[k], fd)
+    checked = []
+    for k in np.argsort(-np.abs(grad))[:4]:
+        fd, eps, fds = O.stable_central_difference(lambda e: oracle_loss(g.amps0 + e * np.eye(16)[k]))
+        if fd is None:
+            continue
+        assert abs(grad[k] - fd) <= 1e-3 * abs(fd), (k, grad[k], fd, eps, fds)
+        checked.append(k)
+        if len(checked) == 2:
+            break
+    assert len(checked) == 2, checked
