@@ -742,7 +742,7 @@ def rt_grad_leg(args):
         _, grad = gs.gradient()
         threads = os.cpu_count() or 1
         t0 = time.perf_counter()
-        comps = []
+        comps, unstable = [], []
 
         def oracle_loss(amps):
             pos = scenes.rt_displace(gs.pos_ref_host, amps, gs.waves, cf.domain_size)
@@ -751,16 +751,17 @@ def rt_grad_leg(args):
         for k in np.argsort(-np.abs(grad))[:4]:
             fd, e, fds = O.stable_central_difference(lambda x: oracle_loss(gs.amps0 + x * np.eye(16)[int(k)]))
             if fd is None:
+                unstable.append({"k": int(k), "grad": float(grad[k]), "fd_ladder": fds})
                 continue
             comps.append({"k": int(k), "grad": float(grad[k]), "fd": fd, "eps": e, "fd_ladder": fds,
                           "rel_err": abs(grad[k] - fd) / abs(fd)})
             if len(comps) == 2:
                 break
         out["fd_check"] = {"res": fr, "steps": fsteps, "oracle": "binary64, solve to 1e-12",
-                           "method": "central differences at eps 1e-5, 3e-6, 1e-6, 3e-7; a component is checked "
+                           "method": "central differences at eps 1e-6, 3e-7, 1e-7, 3e-8, 1e-8; a component is checked "
                                      "at the first two consecutive steps that agree to 2e-4 (away from the jumps "
                                      "that flipping liquid tags and masks put into the loss)",
-                           "components": comps,
+                           "components": comps, "no_stable_difference": unstable,
                            "max_rel_err": max(c["rel_err"] for c in comps) if comps else None,
                            "cpu_s": time.perf_counter() - t0, "threads": threads}
         del gs

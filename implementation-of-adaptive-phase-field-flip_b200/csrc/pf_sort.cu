@@ -121,35 +121,74 @@ __global__ void k_scatter_rank(long long n, const int2* __restrict__ key_rank, c
 // c0 + i (one coalesced pair of loads for the batch), then the warp walks the
 // batch, writing the sorted keys of each cell and ranking its segment, with the
 // next cell's segment loaded while the current one is checked.
-__device__ __forceinline__ void fix_segment(int s, int len, int v, int c, int lane, int* __restrict__ perm,
-                                            int* __restrict__ keys_out) {
-  for (int t = s + lane; t < s + len; t += 32) keys_out[t] = c;
-  if (len <= 1) return;
-  if (len <= 32) {
-    // already ascending?  (the common case: arrivals were in order)
-    const int nxt = __shfl_down_sync(0xffffffffu, v, 1);
-    const bool ok = (lane >= len - 1) || (v < nxt);
-    if (__all_sync(0xffffffffu, ok)) return;
+// number of the n ascending values of a below v
+__device__ __forceinline__ int count_below(const int* a, int n, int v) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] < v) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// A long segment (more than 32 particles in one cell, in arrival order) made
+// ascending by the warp: 32-element chunks are ranked in registers, then runs
+// are merged pairwise (each element's output slot is its index in its own run
+// plus its count in the other run; the values are distinct), ping-ponging with
+// the segment's own keys_out slots, which receive the cell key only afterwards.
+// O(len log^2 len / 32) steps per lane: bounded however many particles share
+// the cell.  a and b are not restrict: lanes read what others wrote before the
+// __syncwarp.
+__device__ void sort_long_segment(int* a, int* b, int len, int lane) {
+  for (int c0 = 0; c0 < len; c0 += 32) {
+    const int m = min(32, len - c0);
+    const int v = lane < m ? a[c0 + lane] : INT_MAX;
     int rank = 0;
-    for (int q = 0; q < len; ++q) rank += (__shfl_sync(0xffffffffu, v, q) < v);
+    for (int q = 0; q < m; ++q) rank += (__shfl_sync(0xffffffffu, v, q) < v);
     __syncwarp();
-    if (lane < len) perm[s + rank] = v;
-  } else {
-    // long segment (> 32 particles in one cell): insertion sort by one lane.
-    // Arrivals are nearly ascending, so this is close to linear in practice.
-    if (lane == 0) {
-      for (int t = s + 1; t < s + len; ++t) {
-        const int w = perm[t];
-        int u = t - 1;
-        while (u >= s && perm[u] > w) {
-          perm[u + 1] = perm[u];
-          --u;
-        }
-        perm[u + 1] = w;
+    if (lane < m) a[c0 + rank] = v;
+    __syncwarp();
+  }
+  int* src = a;
+  int* dst = b;
+  for (long long w2 = 32; w2 < len; w2 *= 2) {
+    const int w = (int)w2;
+    for (long long r = 0; r < len; r += 2 * w2) {
+      const int r0 = (int)r;
+      const int na = min(w, len - r0), nb = max(0, min(w, len - r0 - w));
+      const int* A = src + r0;
+      const int* B = A + na;
+      for (int t = lane; t < na + nb; t += 32) {
+        const bool in_a = t < na;
+        const int v = in_a ? A[t] : B[t - na];
+        const int pos = in_a ? t + count_below(B, nb, v) : (t - na) + count_below(A, na, v);
+        dst[r0 + pos] = v;
       }
     }
     __syncwarp();
+    int* tmp = src;
+    src = dst;
+    dst = tmp;
   }
+  if (src != a)
+    for (int t = lane; t < len; t += 32) a[t] = src[t];
+  __syncwarp();
+}
+
+__device__ __forceinline__ void fix_segment(int s, int len, int v, int c, int lane, int* __restrict__ perm,
+                                            int* __restrict__ keys_out) {
+  if (len > 32) sort_long_segment(perm + s, keys_out + s, len, lane);
+  for (int t = s + lane; t < s + len; t += 32) keys_out[t] = c;
+  if (len <= 1 || len > 32) return;
+  // already ascending?  (the common case: arrivals were in order)
+  const int nxt = __shfl_down_sync(0xffffffffu, v, 1);
+  const bool ok = (lane >= len - 1) || (v < nxt);
+  if (__all_sync(0xffffffffu, ok)) return;
+  int rank = 0;
+  for (int q = 0; q < len; ++q) rank += (__shfl_sync(0xffffffffu, v, q) < v);
+  __syncwarp();
+  if (lane < len) perm[s + rank] = v;
 }
 
 __global__ void k_fix_order(int ncells, const int* __restrict__ start, int* __restrict__ perm,

@@ -494,7 +494,7 @@ def rt_interface_variance(cfg, pos, ptype, dt, steps, nthreads=1):
     return float(((h - h.mean()) ** 2).mean())
 
 
-def stable_central_difference(loss, eps_list=(1e-5, 3e-6, 1e-6, 3e-7), rtol=2e-4):
+def stable_central_difference(loss, eps_list=(1e-6, 3e-7, 1e-7, 3e-8, 1e-8), rtol=2e-4):
     """Central difference (loss(+e) - loss(-e)) / 2e of a scalar function of one
     step size e, taken away from the function's jumps and kinks: the first two
     consecutive step sizes of ``eps_list`` whose differences agree to ``rtol``

@@ -70,7 +70,7 @@ def _near_faces(rng, res, dx, n):
 
 
 @pytest.mark.parametrize("case", ["random", "dam_break", "clustered", "walls", "empty", "one_cell", "faces",
-                                  "faces_odd_dx"])
+                                  "faces_odd_dx", "one_cell_200k"])
 def test_sort_bit_exact(case):
     rng = np.random.default_rng(11)
     res, dx = (24, 20, 36), np.float32(1 / 24)
@@ -98,10 +98,18 @@ def test_sort_bit_exact(case):
         pos[1500:2000] = 7.0
     elif case == "empty":
         pos = np.zeros((0, 3), np.float32)
+    elif case == "one_cell_200k":  # one cell holds 200,000 particles in random order, beside a sparse grid
+        inner = (np.array([3, 4, 5]) + rng.random((200_000, 3))) * float(dx)
+        pos = np.concatenate([inner, rng.random((5000, 3)) * L]).astype(np.float32)
+        pos = pos[rng.permutation(len(pos))]
     else:
         pos = np.full((777, 3), 0.5 * float(dx), np.float32)
     vel = rng.standard_normal(pos.shape).astype(np.float32)
+    import time
+
+    t0 = time.perf_counter()
     keys, perm, start, po, vo = gpu_sort(pos, vel, res, dx)
+    assert time.perf_counter() - t0 < 10.0  # the long segment's order fix is bounded work
     k_ref, p_ref, s_ref = O.sort_by_cell(pos, dx, res)
     assert np.array_equal(start, s_ref)
     assert np.array_equal(perm, p_ref)
