@@ -497,58 +497,50 @@ __device__ __forceinline__ void tma_tile_sweep(float* sP, const BS* sB, const FS
     __syncthreads();
   }
 
-  // relax the cell at coefficient-frame coordinates (q, r, c), c = k - (k0 - 1)
-  auto relax = [&](int q, int r, int c) {
-    float* pp = sP + ((q + 1) * D::PJ + (r + 1)) * TM_W + (c + TM_X0 - 1);
-    const int ce = (q * D::CJ + r) * FW + (c + FX0 - 1);
-    const float bxl = ldT(sX + ce), bxu = ldT(sX + ce + D::CJ * FW);
-    const int ye = (q * (D::CJ + 1) + r) * FW + (c + FX0 - 1);
-    const float byl = ldT(sY + ye), byu = ldT(sY + ye + FW);
-    const float bzl = ldT(sZ + ce), bzu = ldT(sZ + ce + 1);
-    const float bb = ldT(sB + (q * D::CJ + r) * BW + (c + BX0 - 1)) * bsc;
-    bool ok;
-    const float v = gs_update(*pp, pp[-D::PJ * TM_W], pp[D::PJ * TM_W], pp[-TM_W], pp[TM_W], pp[-1], pp[1], bxl, bxu,
-                              byl, byu, bzl, bzu, bb, a.omega, a.flux, &ok);
-    if (ok) *pp = v;
+  // Relax the cells of colour `col` in column (r, c) of the coefficient frame
+  // (cell (q, r, c) is (i0 - 1 + q, j0 - 1 + r, k0 - 1 + c)), planes
+  // qlo <= q < qhi.  Along a column the colour alternates with q, so the
+  // column's cells of one colour are every other plane: the plane steps are
+  // compile-time offsets into the staged boxes.
+  auto relax_column = [&](int r, int c, int qlo, int qhi, int col) {
+    const int j = j0 - 1 + r, k = k0 - 1 + c;
+    if (j < 0 || j >= n1 || k < 0 || k >= n2) return;
+    const int q0 = qlo + ((col - (i0 - 1 + qlo) - j - k) & 1);
+    float* pp = sP + ((q0 + 1) * D::PJ + (r + 1)) * TM_W + (c + TM_X0 - 1);
+    const int cf = (q0 * D::CJ + r) * FW + (c + FX0 - 1);
+    const FS* px = sX + cf;
+    const FS* pz = sZ + cf;
+    const FS* py = sY + (q0 * (D::CJ + 1) + r) * FW + (c + FX0 - 1);
+    const BS* pb = sB + (q0 * D::CJ + r) * BW + (c + BX0 - 1);
+#pragma unroll
+    for (int u = 0; u < (D::CI + 1) / 2; ++u) {
+      const int q = q0 + 2 * u, i = i0 - 1 + q;
+      if (q < qhi && i >= 0 && i < n0) {
+        float* P = pp + u * 2 * D::PJ * TM_W;
+        const FS* X = px + u * 2 * D::CJ * FW;
+        const FS* Y = py + u * 2 * (D::CJ + 1) * FW;
+        const FS* Z = pz + u * 2 * D::CJ * FW;
+        const float bb = ldT(pb + u * 2 * D::CJ * BW) * bsc;
+        bool ok;
+        const float v = gs_update(*P, P[-D::PJ * TM_W], P[D::PJ * TM_W], P[-TM_W], P[TM_W], P[-1], P[1], ldT(X),
+                                  ldT(X + D::CJ * FW), ldT(Y), ldT(Y + FW), ldT(Z), ldT(Z + 1), bb, a.omega, a.flux,
+                                  &ok);
+        if (ok) *P = v;
+      }
+    }
   };
   const int c1 = a.first_color, c2 = c1 ^ 1;
-  // colour 1 on the tile and its 1-cell ring.  Ring row (q, r) holds 34 cells
-  // k0-1 .. k0+32; the 16 of colour c1 inside k0 .. k0+31 go to the 16 lanes
-  // of a half-warp, and the one at k0-1 or k0+32 (the two have opposite
-  // colours) to one thread per row.
-  {
-    constexpr int ROWS = D::CI * D::CJ;
-    const int h = tid & 15;
-    for (int row = tid >> 4; row < ROWS; row += NT / 16) {
-      const int q = row / D::CJ, r = row - q * D::CJ;
-      const int i = i0 - 1 + q, j = j0 - 1 + r;
-      const int par = (c1 - i - j - k0) & 1;
-      const int c = 1 + 2 * h + par, k = k0 - 1 + c;
-      if (i < 0 || i >= n0 || j < 0 || j >= n1 || k >= n2) continue;
-      relax(q, r, c);
-    }
-    for (int row = tid; row < ROWS; row += NT) {
-      const int q = row / D::CJ, r = row - q * D::CJ;
-      const int i = i0 - 1 + q, j = j0 - 1 + r;
-      const bool lower = ((c1 - i - j - (k0 - 1)) & 1) == 0;  // k0-1 has colour c1
-      const int c = lower ? 0 : SW_TK + 1, k = k0 - 1 + c;
-      if (i < 0 || i >= n0 || j < 0 || j >= n1 || k < 0 || k >= n2) continue;
-      relax(q, r, c);
-    }
+  // colour 1 on the tile and its 1-cell ring: columns (r, c) of the
+  // CJ x (SW_TK + 2) frame, planes 0 .. CI-1
+  for (int t = tid; t < D::CJ * (SW_TK + 2); t += NT) {
+    const int r = t / (SW_TK + 2), c = t - r * (SW_TK + 2);
+    relax_column(r, c, 0, D::CI, c1);
   }
   __syncthreads();
-  // colour 2 on the tile: 16 cells of the colour per row, a half-warp per row
-  {
-    constexpr int ROWS = TI * SW_TJ;
-    const int h = tid & 15;
-    for (int row = tid >> 4; row < ROWS; row += NT / 16) {
-      const int q = row >> 3, r = row & 7;  // SW_TJ == 8
-      const int i = i0 + q, j = j0 + r;
-      const int par = (c2 - i - j - k0) & 1;
-      const int c = 2 * h + par, k = k0 + c;
-      if (i >= n0 || j >= n1 || k >= n2) continue;
-      relax(q + 1, r + 1, c + 1);
-    }
+  // colour 2 on the tile: columns (1 .. SW_TJ, 1 .. SW_TK), planes 1 .. TI
+  for (int t = tid; t < SW_TJ * SW_TK; t += NT) {
+    const int r = 1 + (t >> 5), c = 1 + (t & 31);  // SW_TK == 32
+    relax_column(r, c, 1, TI + 1, c2);
   }
   __syncthreads();
   for (int e = tid; e < TI * SW_TJ * SW_TK; e += NT) {

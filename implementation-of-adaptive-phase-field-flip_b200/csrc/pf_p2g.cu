@@ -215,17 +215,26 @@ __device__ __forceinline__ void p2g_grid(const P2GArgs& a, float* acc, int i, in
   Box<G> box;
   box.zero();
   const float ci = (float)i, cj = (float)j, ck = (float)k;
-  // one particle of prefetch: the loads of t+1 are in flight while t is splatted
-  float4 Pn = make_float4(0.f, 0.f, 0.f, 0.f), Vn = Pn;
+  // two particles of prefetch: the loads of t+2 are in flight while t is
+  // splatted (a warp holds too few peers on its SM to hide an L2 round trip
+  // behind one particle's arithmetic)
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 Pa = z4, Va = z4, Pb = z4, Vb = z4;
   if (s < e) {
-    Pn = __ldg(a.pos + s);
-    if (G < 3) Vn = __ldg(a.vel + s);
+    Pa = __ldg(a.pos + s);
+    if (G < 3) Va = __ldg(a.vel + s);
+  }
+  if (s + 1 < e) {
+    Pb = __ldg(a.pos + s + 1);
+    if (G < 3) Vb = __ldg(a.vel + s + 1);
   }
   for (int t = s; t < e; ++t) {
-    const float4 P = Pn, V = Vn;
-    if (t + 1 < e) {
-      Pn = __ldg(a.pos + t + 1);
-      if (G < 3) Vn = __ldg(a.vel + t + 1);
+    const float4 P = Pa, V = Va;
+    Pa = Pb;
+    Va = Vb;
+    if (t + 2 < e) {
+      Pb = __ldg(a.pos + t + 2);
+      if (G < 3) Vb = __ldg(a.vel + t + 2);
     }
     const int flags = __float_as_int(P.w);
     if ((flags >> PF_PSTATE_SHIFT) & 3) continue;  // droplets / dead particles do not splat
@@ -239,7 +248,7 @@ __device__ __forceinline__ void p2g_grid(const P2GArgs& a, float* acc, int i, in
   box.flush(acc + a1 * PG_BOX, acc + a2 * PG_BOX, li, lj, lane);
 }
 
-__global__ void __launch_bounds__(PG_NT) k_p2g(const __grid_constant__ P2GArgs a) {
+__global__ void __launch_bounds__(PG_NT, 2) k_p2g(const __grid_constant__ P2GArgs a) {
   extern __shared__ __align__(16) float acc[];  // [PG_NACC][PG_BOX]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int k0 = blockIdx.x * PG_TK, j0 = blockIdx.y * PG_TJ, i0 = blockIdx.z * PG_TI;
