@@ -233,9 +233,13 @@ __global__ void __launch_bounds__(128) k_adj_g2p_advect(AdjG2PArgs a) {
         }
       }
     }
-    // ---- reverse: RK3 (gx is now the adjoint of the unclamped update)
+    // ---- reverse: RK3 (gx is now the adjoint of the unclamped update).  An
+    // air particle's first stage samples u at x, exactly as its G2P does: its
+    // adjoint joins the G2P adjoint's u taps below (one scatter, one gradient)
+    const bool merge_k1 = rk && a.do_g2p && !liquid;
+    float gk1[3] = {0.f, 0.f, 0.f};
     if (rk) {
-      float gk1[3], gk2[3], gk3[3], gy[3];
+      float gk2[3], gk3[3], gy[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         gk1[c] = a.dt * c1 * gx[c];
@@ -254,23 +258,26 @@ __global__ void __launch_bounds__(128) k_adj_g2p_advect(AdjG2PArgs a) {
         gx[c] += gy[c];
         gk1[c] += h1 * gy[c];
       }
-      sample_vec_adjoint(F, FB, x, a.inv_dx, a.nx, a.ny, a.nz, gk1, gy);
+      if (!merge_k1) {
+        sample_vec_adjoint(F, FB, x, a.inv_dx, a.nx, a.ny, a.nz, gk1, gy);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) gx[c] += gy[c];
+        for (int c = 0; c < 3; ++c) gx[c] += gy[c];
+      }
     }
     // ---- reverse: G2P, v' = alpha v + I(u) - alpha I(u*)
     if (a.do_g2p && pstate == 0) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const float g = gv[c];
+        const float gu = merge_k1 ? g + gk1[c] : g;  // adjoint of I(u)(x)
         TapFrame fr;
         tap_frame(x, a.inv_dx, a.nx, a.ny, a.nz, c, fr);
         float gr_u[3], gr_s[3];
         sample_grad(a.u[c], c, fr, a.ny, a.nz, a.inv_dx, gr_u);
         sample_grad(a.us[c], c, fr, a.ny, a.nz, a.inv_dx, gr_s);
 #pragma unroll
-        for (int d = 0; d < 3; ++d) gx[d] += g * gr_u[d] - alpha * g * gr_s[d];
-        scatter_taps(a.gu[c], c, fr, a.ny, a.nz, g);
+        for (int d = 0; d < 3; ++d) gx[d] += gu * gr_u[d] - alpha * g * gr_s[d];
+        scatter_taps(a.gu[c], c, fr, a.ny, a.nz, gu);
         scatter_taps(a.gus[c], c, fr, a.ny, a.nz, -alpha * g);
         gv[c] = alpha * g;
       }

@@ -2399,7 +2399,16 @@ int launch_sweep(pf_mg_plan* P, int lv, const T* p_in, bool zero_in, T* p_out, c
   if constexpr (!std::is_same<T, float>::value) {
     TileMaps maps;
     constexpr bool B32 = std::is_same<TB, float>::value;
-    if (P->use_tma && L.nx >= 128 && tma_maps16<8, T, TB>(P, lv, p_in, b, V, &maps)) {
+    // as in FP32: six-plane tiles at 128+ planes (68 KB with the FP32 b rows
+    // of the finest level: three CTAs per SM), eight-plane tiles at 64 planes
+    if (P->use_tma && L.nx >= 128 && tma_maps16<6, T, TB>(P, lv, p_in, b, V, &maps)) {
+      const dim3 g6(grid.x, grid.y, (L.nx + 5) / 6);
+      PF_CUDA_TRY(launch_overlapped(k_rb_tile_tma16<6, 512, T, TB>, g6, dim3(512), Tma16Dims<6, B32>::SMEM, s, maps,
+                                    a));
+      PF_LAUNCHED();
+      return PF_OK;
+    }
+    if (P->use_tma && L.nx >= 64 && tma_maps16<8, T, TB>(P, lv, p_in, b, V, &maps)) {
       const dim3 g8(grid.x, grid.y, (L.nx + 7) / 8);
       PF_CUDA_TRY(launch_overlapped(k_rb_tile_tma16<8, 512, T, TB>, g8, dim3(512), Tma16Dims<8, B32>::SMEM, s, maps,
                                     a));
@@ -2838,6 +2847,10 @@ template <class T> cudaError_t set_smem_attrs() {
                              (int)Tma16Dims<4, true>::SMEM));
     chk(cudaFuncSetAttribute(k_rb_tile_tma16<4, SW_NT, T, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)Tma16Dims<4, false>::SMEM));
+    chk(cudaFuncSetAttribute(k_rb_tile_tma16<6, 512, T, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)Tma16Dims<6, true>::SMEM));
+    chk(cudaFuncSetAttribute(k_rb_tile_tma16<6, 512, T, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)Tma16Dims<6, false>::SMEM));
     chk(cudaFuncSetAttribute(k_rb_tile_tma16<8, 512, T, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)Tma16Dims<8, true>::SMEM));
     chk(cudaFuncSetAttribute(k_rb_tile_tma16<8, 512, T, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,

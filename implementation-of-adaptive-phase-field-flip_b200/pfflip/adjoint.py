@@ -152,31 +152,54 @@ class DiffSim:
             self.sim.step(self.dt)
         return self._to_ids(self.sim._pos4), self._to_ids(self.sim._vel4)
 
+    def _saved_fields(self):
+        s = self.sim
+        return [as_tensor(a) for a in (*s.vel, *s.vel_star, *s.vel_liq, *s.beta, *s.mass, *s.mom, s.is_liquid,
+                                        s.pressure)]
+
+    def _snapshot(self):
+        """Everything the step's adjoint reads, right after its grid stages: the
+        sorted particles, the sort permutation and the grid fields."""
+        s = self.sim
+        return (s._pos4.clone(), s._vel4.clone(), s._perm.clone(), [t.clone() for t in self._saved_fields()])
+
+    def _restore(self, snap):
+        s = self.sim
+        p4, v4, perm, fields = snap
+        s._pos4.copy_(p4)
+        s._vel4.copy_(v4)
+        s._perm.copy_(perm)
+        for t, src in zip(self._saved_fields(), fields):
+            t.copy_(src)
+        s.solver.build_hierarchy(*s.beta)  # the adjoint solve uses this step's operator
+        s._particles_changed()
+
     def _backward_block(self, x, v, nsteps, gx, gv):
+        """Replay the block once, keeping each step's grid state (its sorted
+        particles, permutation and fields: about 0.1 GB per step at 64^3 / 8
+        ppc), then walk the steps in reverse, restoring that state for each
+        step's adjoint instead of recomputing the step's grid stages."""
         s = self.sim
         self._load(x, v)
-        states = []
+        s._particles_changed()  # step 0 sorts again (the identity), so its permutation maps onto this order
+        snaps = []
         for _ in range(nsteps):
-            states.append((s._pos4.clone(), s._vel4.clone()))
-            s.step(self.dt)
+            self._grid_stages()
+            snaps.append(self._snapshot())
+            s._g2p_advect(self.dt, do_g2p=True, do_advect=True)
         ga, gb = self._g4[0], self._g4[1]
         self._from_ids(gx, ga)
         self._from_ids(gv, gb)
         for k in range(nsteps - 1, -1, -1):
-            p0, v0 = states[k]
-            s._pos4.copy_(p0)
-            s._particles_changed()
-            s._vel4.copy_(v0)
-            self._grid_stages()
+            self._restore(snaps[k])
+            snaps[k] = None
             # ga/gb are in the order of the arrays after the step, which is the
             # order after the step's sort; the result is in the order before it
             nxt_p, nxt_v = torch.empty_like(ga), torch.empty_like(gb)
             self._step_adjoint(ga, gb, nxt_p, nxt_v)
             ga, gb = nxt_p, nxt_v
-            s._pos4.copy_(p0)
-            s._particles_changed()
-            s._vel4.copy_(v0)
-        # the arrays now hold the block's first state, in the order ga/gb use
+        # step 0's sort was the identity on the loaded order, so the snapshot's
+        # ids give the order ga/gb use
         return self._to_ids(ga), self._to_ids(gb)
 
     def rollout(self, x, v, steps: int):

@@ -262,7 +262,7 @@ class Simulator:
         self._fresh_sort = True
         self._vmax_valid = False
 
-    def read_particles(self, pos_out=None, vel_out=None):
+    def read_particles(self, pos_out=None, vel_out=None, sync=True):
         """Positions and velocities in the original order, copied into the given
         (pinned) host tensors when provided; returns (pos, vel).
 
@@ -270,7 +270,15 @@ class Simulator:
         stream in chunks of _CHUNK bytes, the positions' copy overlapping the
         reordering of the velocities; the caller's stream waits for both.  The
         chunks' events stay recorded, so that a set_particles from these same
-        host buffers uploads each chunk as soon as its download has landed."""
+        host buffers uploads each chunk as soon as its download has landed.
+
+        sync=True (the default) returns only once the host tensors hold the
+        values, as the reference's synchronous read does.  sync=False returns
+        as soon as the copies are queued: the host must not read pos_out or
+        vel_out before torch.cuda.synchronize() (or the caller's stream) says
+        they have landed; handing them straight back to set_particles is safe,
+        which is what lets a host round trip per step overlap its uploads with
+        the downloads."""
         ids = self._ids().long()
         main = torch.cuda.current_stream(self.dev)
         out = []
@@ -300,6 +308,8 @@ class Simulator:
                 out.append(dst)
         if copied:
             main.wait_stream(self._copy_streams()[0])
+            if sync:
+                self._copy_streams()[0].synchronize()
         self._pending_d2h = pending
         return tuple(out)
 

@@ -269,9 +269,7 @@ def test_host_round_trip_with_overlapped_copies_is_exact(monkeypatch):
             sim._vel4[:, :3] *= 1.5
             if not sync:
                 torch.cuda._sleep(20_000_000)  # ~10 ms: the next uploads are queued before these downloads run
-            sim.read_particles(hp, hv)
-            if sync:
-                torch.cuda.synchronize()
+            sim.read_particles(hp, hv, sync=sync)
         torch.cuda.synchronize()
         assert np.array_equal(hp.numpy(), exp_p), sync
         assert np.array_equal(hv.numpy(), exp_v), sync
@@ -292,7 +290,7 @@ def test_host_round_trip_steps_read_back_the_device_state():
     for _ in range(3):
         sim.set_particles(hp, hv, ht)
         sim.step(dt)
-        sim.read_particles(hp, hv)
+        sim.read_particles(hp, hv, sync=False)
     torch.cuda.synchronize()
     assert np.array_equal(hp.numpy(), sim.px.numpy()) and np.array_equal(hv.numpy(), sim.pv.numpy())
     assert np.abs(hp.numpy() - pos).max() > 0
