@@ -9,7 +9,8 @@
 //   4. per-cell order fix: the ranks of one cell follow arrival order; one
 //      warp per cell ranks the original indices so each cell's segment is
 //      ascending, which is exactly a stable sort; sorted keys are written here
-//   5. gather of the two float4 particle streams through perm
+//   5. gather of the two float4 particle streams through perm, by the same
+//      warp right after each cell's fix (one kernel for 4 and 5)
 //
 // Bytes per particle: 16 (pos) + 8 (key, rank) in pass 1, 8 + 4 in pass 3,
 // 12 in pass 4, 4 + 32 + 32 in pass 5, plus 8 per cell for the scan.
@@ -176,23 +177,52 @@ __device__ void sort_long_segment(int* a, int* b, int len, int lane) {
   __syncwarp();
 }
 
-__device__ __forceinline__ void fix_segment(int s, int len, int v, int c, int lane, int* __restrict__ perm,
-                                            int* __restrict__ keys_out) {
-  if (len > 32) sort_long_segment(perm + s, keys_out + s, len, lane);
-  for (int t = s + lane; t < s + len; t += 32) keys_out[t] = c;
-  if (len <= 1 || len > 32) return;
+// Passes 4 and 5 in one.  A cell's segment of perm holds its particles in
+// arrival order; the warp puts it in index order (which is exactly the stable
+// sort), writes the cell's sorted keys, and copies the segment's particles --
+// both float4 streams -- to their sorted slots, so perm is read once and the
+// writes of a segment are contiguous.  Segments of up to 32 particles are
+// ranked in registers (most arrive in order already); longer ones take the
+// warp merge sort above.
+__device__ __forceinline__ void fix_gather_segment(int s, int len, int v, int c, int lane, int* __restrict__ perm,
+                                                   int* __restrict__ keys_out, const float4* __restrict__ pin,
+                                                   const float4* __restrict__ vin, float4* __restrict__ pout,
+                                                   float4* __restrict__ vout) {
+  if (len > 32) {
+    sort_long_segment(perm + s, keys_out + s, len, lane);
+    for (int t = lane; t < len; t += 32) {
+      keys_out[s + t] = c;
+      const int p = perm[s + t];
+      pout[s + t] = __ldg(pin + p);
+      vout[s + t] = __ldg(vin + p);
+    }
+    return;
+  }
+  if (len == 0) return;
   // already ascending?  (the common case: arrivals were in order)
   const int nxt = __shfl_down_sync(0xffffffffu, v, 1);
   const bool ok = (lane >= len - 1) || (v < nxt);
-  if (__all_sync(0xffffffffu, ok)) return;
-  int rank = 0;
-  for (int q = 0; q < len; ++q) rank += (__shfl_sync(0xffffffffu, v, q) < v);
-  __syncwarp();
-  if (lane < len) perm[s + rank] = v;
+  int slot = lane;
+  if (!__all_sync(0xffffffffu, ok)) {
+    int rank = 0;
+    for (int q = 0; q < len; ++q) rank += (__shfl_sync(0xffffffffu, v, q) < v);
+    slot = rank;
+    if (lane < len) perm[s + rank] = v;
+  }
+  if (lane < len) {
+    keys_out[s + lane] = c;
+    pout[s + slot] = __ldg(pin + v);
+    vout[s + slot] = __ldg(vin + v);
+  }
 }
 
-__global__ void k_fix_order(int ncells, const int* __restrict__ start, int* __restrict__ perm,
-                            int* __restrict__ keys_out) {
+// One warp per batch of 32 consecutive cells: lane i loads the bounds of cell
+// c0 + i (one coalesced pair of loads for the batch), then the warp walks the
+// batch, the next cell's segment loaded while the current one is ordered and
+// copied.
+__global__ void k_fix_gather(int ncells, const int* __restrict__ start, int* __restrict__ perm,
+                             int* __restrict__ keys_out, const float4* __restrict__ pin,
+                             const float4* __restrict__ vin, float4* __restrict__ pout, float4* __restrict__ vout) {
   const int lane = threadIdx.x & 31;
   const int nbatch = (ncells + 31) >> 5;
   const int warps = (gridDim.x * blockDim.x) >> 5;
@@ -204,25 +234,16 @@ __global__ void k_fix_order(int ncells, const int* __restrict__ start, int* __re
     int v = (lane < len && len <= 32) ? perm[s + lane] : INT_MAX;
     for (int q = 0; q < nb; ++q) {
       int s2 = 0, len2 = 0, v2 = INT_MAX;
-      if (q + 1 < nb) {  // the next cell's segment, in flight while this one is checked
+      if (q + 1 < nb) {  // the next cell's segment, in flight while this one is handled
         s2 = __shfl_sync(0xffffffffu, my_s, q + 1);
         len2 = __shfl_sync(0xffffffffu, my_e, q + 1) - s2;
         v2 = (lane < len2 && len2 <= 32) ? perm[s2 + lane] : INT_MAX;
       }
-      fix_segment(s, len, v, c0 + q, lane, perm, keys_out);
+      fix_gather_segment(s, len, v, c0 + q, lane, perm, keys_out, pin, vin, pout, vout);
       s = s2;
       len = len2;
       v = v2;
     }
-  }
-}
-
-__global__ void k_gather(long long n, const int* __restrict__ perm, const float4* __restrict__ pin,
-                         const float4* __restrict__ vin, float4* __restrict__ pout, float4* __restrict__ vout) {
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    const int p = perm[t];
-    pout[t] = __ldg(pin + p);
-    vout[t] = __ldg(vin + p);
   }
 }
 
@@ -257,12 +278,10 @@ int sort_from_keys(const pf_grid* g, int64_t n, const int2* key_rank, int* sums,
   if (n == 0) return PF_OK;
   k_scatter_rank<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, key_rank, cell_start, perm_out);
   PF_LAUNCHED();
-  k_fix_order<<<grid_for(nc, 256, 1 << 20), 256, 0, s>>>((int)nc, cell_start, perm_out, keys_out);
-  PF_LAUNCHED();
-  k_gather<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(n, perm_out, reinterpret_cast<const float4*>(pos4_in),
-                                                          reinterpret_cast<const float4*>(vel4_in),
-                                                          reinterpret_cast<float4*>(pos4_out),
-                                                          reinterpret_cast<float4*>(vel4_out));
+  k_fix_gather<<<grid_for(nc, 256, 1 << 20), 256, 0, s>>>(
+      (int)nc, cell_start, perm_out, keys_out, reinterpret_cast<const float4*>(pos4_in),
+      reinterpret_cast<const float4*>(vel4_in), reinterpret_cast<float4*>(pos4_out),
+      reinterpret_cast<float4*>(vel4_out));
   PF_LAUNCHED();
   return PF_OK;
 }
