@@ -107,7 +107,7 @@ __global__ void k_scan_add(long long n, int* __restrict__ a, const int* __restri
 
 // ---------------------------------------------------------------- scatter + order fix
 // pass 3: perm[start[key] + rank] = p; the slots of one cell are then in
-// arrival order, which k_fix_order turns into index order
+// arrival order, which k_fix_gather turns into index order
 __global__ void k_scatter_rank(long long n, const int2* __restrict__ key_rank, const int* __restrict__ start,
                                int* __restrict__ perm) {
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
