@@ -114,6 +114,9 @@ class ParticleField:
             dst = s._pos4 if k == "pos" else s._vel4
             dst[:, :3] = t.reshape(-1, 3).to(torch.float32)[ids]
             return self
+        if k == "pdrop_r":
+            s._drop_r[:] = t.reshape(-1).to(torch.float32)[ids]
+            return self
         if k not in ("ptype", "pstate"):
             raise TypeError(f"{k} is derived from the particle type and cannot be assigned")
         flags = s._flags()

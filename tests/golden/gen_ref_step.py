@@ -84,8 +84,12 @@ class Array:
 def make_warp_module():
     wp = types.ModuleType("warp")
     wp.__doc__ = "binary32 scalar stand-in for NVIDIA Warp (test fixture generation only)"
+    class Float16Type(_DType):
+        def __call__(self, x):
+            return np.float16(F32(x))
+
     wp.float32 = _DType("float32", np.float32)
-    wp.float16 = _DType("float16", np.float16)
+    wp.float16 = Float16Type("float16", np.float16)
     wp.int32 = _DType("int32", np.int32)
     wp.uint32 = _DType("uint32", np.uint32)
 
@@ -159,6 +163,32 @@ def make_warp_module():
         return np.sqrt(F32(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]))
 
     wp.length = length
+    wp.exp = lambda x: np.exp(F32(x))
+
+    # Warp's random stream (rand_init/randf/randn) is replaced by the stream
+    # the library documents for its droplet radii and spray emission: the
+    # PCG-RXS-M-XS 32-bit hash seeded with hash(hash(seed) + id), uniforms
+    # ((s >> 8) + 0.5) * 2^-24, normals by Box-Muller, in binary32.  Every
+    # other line of the droplet kernels is the reference's own.
+    def pcg_hash(v):
+        s = (v * 747796405 + 2891336453) & 0xFFFFFFFF
+        w = (((s >> ((s >> 28) + 4)) ^ s) * 277803737) & 0xFFFFFFFF
+        return (w >> 22) ^ w
+
+    class RandState:
+        def __init__(self, seed, offset):
+            self.s = pcg_hash((pcg_hash(int(seed) & 0xFFFFFFFF) + int(offset)) & 0xFFFFFFFF)
+
+    def randf(rng):
+        rng.s = pcg_hash(rng.s)
+        return F32(F32(F32(rng.s >> 8) + F32(0.5)) * F32(1.0 / 16777216.0))
+
+    def randn(rng):
+        u1 = randf(rng)
+        u2 = randf(rng)
+        return F32(np.sqrt(F32(F32(-2.0) * np.log(u1))) * np.cos(F32(F32(2.0 * math.pi) * u2)))
+
+    wp.rand_init, wp.randf, wp.randn = RandState, randf, randn
 
     def atomic_add(arr, *args):
         *idx, v = args
@@ -319,6 +349,101 @@ def run_case(mods, name, cfg_kw, scene, rng_seed, vel_scale, droplet_every=0):
     return out, cfg_kw
 
 
+def run_droplet_case(mods, name, cfg_kw, rng_seed):
+    """The droplet stage (``pfflip/sim.py:343-392``) and the spray raster
+    (``:394-401``) on an 8^3 dam break whose particles are placed so that every
+    branch runs: liquid particles moved into the air (new droplets), air
+    particles moved into the liquid (bubbles, deleted), droplets moved back
+    into the liquid (merged), droplets in the air with radii near the
+    evaporation limit, droplets leaving through the ceiling, dead particles,
+    and shear spray from the interfacial band with the threshold at the band's
+    median shear."""
+    Config, Simulator, scenes, D = mods["config"].Config, mods["sim"].Simulator, mods["scenes"], mods["droplets"]
+    wp = mods["sim"].wp
+    cfg = Config(**cfg_kw)
+    pos, vel, ptype = scenes.dam_break(cfg)
+    rng = np.random.default_rng(rng_seed)
+    vel = (vel + 1.0 * rng.standard_normal(vel.shape)).astype(np.float32)
+    sim = Simulator(cfg)
+    sim.set_particles(pos, vel, ptype)
+    n = len(pos)
+    pstate = np.zeros(n, np.int32)
+    pstate[5::11] = 1
+    pstate[7::13] = 2
+    sim.pstate.assign(pstate)
+    sim.step_index = 3
+    dt = 0.5 * cfg.dx / math.sqrt(2 * 9.81 * 0.6)
+    sim._p2g()
+    sim._phase_field_and_coefficients()
+    for ax in range(3):
+        sim.vel_star[ax].assign(sim.vel[ax].numpy())
+    sim._add_forces(dt)
+    sim._pressure_solve(dt)
+    sim._project(dt)
+    sim._g2p()
+    sim._extrapolate_liquid_velocity()
+
+    # place particles so that every branch of the stage runs
+    px, pv = sim.px.numpy(), sim.pv.numpy()
+    sx, sy, sz = cfg.domain_size
+    liq_flip = np.flatnonzero((ptype == 1) & (pstate == 0))
+    air_flip = np.flatnonzero((ptype == 0) & (pstate == 0))
+    drops = np.flatnonzero(pstate == 1)
+    a = liq_flip[::5]  # into the air: new droplets
+    px[a] = np.stack([rng.uniform(0.6, 0.9, len(a)) * sx, rng.uniform(0.72, 0.9, len(a)) * sy,
+                      rng.uniform(0.1, 0.9, len(a)) * sz], 1)
+    b = air_flip[::7]  # into the liquid: bubbles
+    px[b] = np.stack([rng.uniform(0.05, 0.3, len(b)) * sx, rng.uniform(0.05, 0.45, len(b)) * sy,
+                      rng.uniform(0.1, 0.9, len(b)) * sz], 1)
+    m = drops[::3]  # droplets back into the liquid: merged
+    px[m] = np.stack([rng.uniform(0.05, 0.3, len(m)) * sx, rng.uniform(0.05, 0.45, len(m)) * sy,
+                      rng.uniform(0.1, 0.9, len(m)) * sz], 1)
+    c = np.setdiff1d(drops, m)  # droplets in the air
+    px[c] = np.stack([rng.uniform(0.55, 0.95, len(c)) * sx, rng.uniform(0.7, 0.95, len(c)) * sy,
+                      rng.uniform(0.05, 0.95, len(c)) * sz], 1)
+    up = c[::4]  # leaving through the ceiling
+    px[up, 1] = sy - 0.2 * cfg.dx
+    pv[up, 1] = 4.0
+    r_min = 0.02 * cfg.dx
+    radii = np.zeros(n, np.float32)
+    radii[drops] = rng.uniform(0.3, 1.5, len(drops)) * cfg.droplet_radius_mean * cfg.dx
+    radii[c[1::4]] = rng.uniform(1.05, 3.0, len(c[1::4])) * r_min  # near the evaporation limit
+    sim.px.assign(px.astype(np.float32))
+    sim.pv.assign(pv.astype(np.float32))
+    sim.pdrop_r.assign(radii)
+
+    # shear threshold: the median shear at the interfacial band's liquid particles
+    wp.launch(D.velocity_gradient_magnitude, dim=sim.res, inputs=[*sim.vel, sim.shear, cfg.dx])
+    shear = sim.shear.numpy()
+    phi = sim.phi_cell.numpy()
+    cell = np.clip((px / cfg.dx).astype(int), 0, np.array(sim.res) - 1)
+    ph = phi[cell[:, 0], cell[:, 1], cell[:, 2]]
+    band = (ptype == 1) & (pstate == 0) & (ph > 0.2) & (ph < 0.8)
+    thr = float(np.median(shear[cell[band, 0], cell[band, 1], cell[band, 2]]))
+    sim.cfg.spray_shear_threshold = thr
+
+    s = {"dt": np.float64(dt), "step_index": np.int64(sim.step_index), "spray_threshold": np.float64(thr)}
+    s["in_px"], s["in_pv"], s["in_ptype"] = sim.px.numpy(), sim.pv.numpy(), sim.ptype.numpy()
+    s["in_pstate"], s["in_pdrop_r"] = sim.pstate.numpy(), sim.pdrop_r.numpy()
+    s["in_phi_cell"] = sim.phi_cell.numpy()
+    for ax in range(3):
+        s[f"in_vel{ax}"] = sim.vel[ax].numpy()
+    sim._droplets(dt)
+    s["out_shear"] = sim.shear.numpy()
+    s["out_px"], s["out_pv"] = sim.px.numpy(), sim.pv.numpy()
+    s["out_pstate"], s["out_pdrop_r"] = sim.pstate.numpy(), sim.pdrop_r.numpy()
+    s["out_counters"] = np.array([sim.droplet_stats[k] for k in ("emitted", "bubbles", "merged", "spray")],
+                                 np.int64)
+    s["spray_density"] = sim.rasterize_spray().numpy()
+    kw = dict(cfg_kw, spray_shear_threshold=thr)
+    return {f"{name}/{k}": v for k, v in s.items()}, kw
+
+
+DROPLET_CASES = [
+    ("droplets_8", dict(res=(8, 8, 8), dx=1.0 / 8, ppc=8, seed=21, droplets=True, pcg_tol=1e-5,
+                        evaporation_k=0.5, spray_emission_rate=0.5, spray_shear_threshold=1.0), 14),
+]
+
 CASES = [
     # the 32^3 workload's form at 8^3: dam break, 8 ppc, perturbed velocities,
     # droplets/dead particles in the stream; tolerance 1e-6 as in that
@@ -348,6 +473,11 @@ def main():
         v, kw = run_case(mods, name, kw, scene, seed, vs, dr)
         allv.update(v)
         meta[name] = {"cfg": kw, "scene": scene}
+        print(name, "done", flush=True)
+    for name, kw, seed in DROPLET_CASES:
+        v, kw = run_droplet_case(mods, name, kw, seed)
+        allv.update(v)
+        meta[name] = {"cfg": kw, "scene": "dam_break"}
         print(name, "done", flush=True)
     allv["meta"] = np.array(repr(meta))
     np.savez_compressed(args.out, **allv)

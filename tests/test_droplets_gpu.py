@@ -150,3 +150,47 @@ def test_full_steps_with_droplets_match_oracle():
     assert bad.sum() <= max(2, int(1e-4 * len(pos)))
     ok = ~bad & (st_g != 2)
     assert np.abs(sim.px.numpy()[ok] - o.px[ok]).max() < 1e-3 * cfg.dx
+
+
+def test_droplet_stage_matches_reference_fixture():
+    """The library's droplet stage and float16 spray raster against the
+    reference's own kernels (tests/golden/ref_step.npz, case droplets_8: an
+    8^3 state where new droplets, bubbles, merges, shear spray, evaporation
+    deaths and ceiling exits all occur; the generator draws the reference's
+    radii from the stream the library documents).  States and counters equal
+    up to threshold rounding; radii within 1e-5 relative; droplet positions
+    and velocities within 1e-5 of their largest value; shear within 1e-5; the
+    raster within 1e-2 of its maximum (float16 atomics in another order)."""
+    import ast
+    import os
+
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_step.npz"))
+    meta = ast.literal_eval(str(d["meta"]))
+    g = lambda k: d[f"droplets_8/{k}"]  # noqa: E731
+    cfg = Config(**meta["droplets_8"]["cfg"], device=DEV)
+    sim = Simulator(cfg)
+    sim.set_particles(g("in_px"), g("in_pv"), g("in_ptype"))
+    sim.pstate.assign(g("in_pstate"))
+    sim.pdrop_r.assign(g("in_pdrop_r"))
+    sim.phi_cell.assign(g("in_phi_cell"))
+    for ax in range(3):
+        sim.vel[ax].assign(g(f"in_vel{ax}"))
+    sim.step_index = int(g("step_index"))
+    sim._droplets(float(g("dt")))
+    sh, sh_ref = sim.shear.numpy(), g("out_shear")
+    assert np.abs(sh - sh_ref).max() <= 1e-5 * np.abs(sh_ref).max()
+    st, st_ref = sim.pstate.numpy(), g("out_pstate")
+    bad = st != st_ref
+    assert bad.sum() <= 2, int(bad.sum())
+    counts = [sim.droplet_stats[k] for k in ("emitted", "bubbles", "merged", "spray")]
+    assert np.abs(np.array(counts) - g("out_counters")).max() <= bad.sum(), (counts, g("out_counters"))
+    drop = (st_ref == 1) & ~bad
+    r, r_ref = sim.pdrop_r.numpy()[drop], g("out_pdrop_r")[drop]
+    assert np.abs(r - r_ref).max() <= 1e-5 * np.abs(r_ref).max()
+    live = (st_ref != 2) & ~bad
+    assert np.abs(sim.px.numpy()[live] - g("out_px")[live]).max() <= 1e-5 * max(cfg.domain_size)
+    pv_ref = g("out_pv")[live]
+    assert np.abs(sim.pv.numpy()[live] - pv_ref).max() <= 1e-5 * np.abs(pv_ref).max()
+    dens = sim.rasterize_spray().numpy().astype(np.float64)
+    ref = g("spray_density").astype(np.float64)
+    assert ref.max() > 0 and np.abs(dens - ref).max() <= 1e-2 * ref.max()
