@@ -348,15 +348,24 @@ class Simulator:
         return d
 
     def _alloc_particles(self, n):
+        # each stream is a view of the first n rows of at least one row of
+        # storage, so that an empty particle set still passes valid device
+        # pointers (the library launches nothing for n = 0)
         dev = self.dev
-        self._drop_r = torch.zeros(n, dtype=torch.float32, device=dev)
-        self._drop_r_alt = torch.empty_like(self._drop_r)
-        self._pos4 = torch.empty((n, 4), dtype=torch.float32, device=dev)
-        self._vel4 = torch.empty((n, 4), dtype=torch.float32, device=dev)
-        self._pos4_alt = torch.empty_like(self._pos4)
-        self._vel4_alt = torch.empty_like(self._vel4)
-        self._keys = torch.empty(n, dtype=torch.int32, device=dev)
-        self._perm = torch.empty(n, dtype=torch.int32, device=dev)
+        m = max(n, 1)
+
+        def rows(*shape, dtype=torch.float32, zero=False):
+            a = (torch.zeros if zero else torch.empty)((m,) + shape, dtype=dtype, device=dev)
+            return a[:n]
+
+        self._drop_r = rows(zero=True)
+        self._drop_r_alt = rows()
+        self._pos4 = rows(4)
+        self._vel4 = rows(4)
+        self._pos4_alt = rows(4)
+        self._vel4_alt = rows(4)
+        self._keys = rows(dtype=torch.int32)
+        self._perm = rows(dtype=torch.int32)
         nc = self.res[0] * self.res[1] * self.res[2]
         self._cell_start = torch.zeros(nc + 1, dtype=torch.int32, device=dev)
         wsb = int(N.lib().pf_sort_workspace_bytes(C.byref(self._g), n))

@@ -352,3 +352,35 @@ def test_frame_loop_matches_oracle(tmp_path):
         fr = io.load_frame(str(tmp_path / f"frame_{f:04d}.npz"))
         assert abs(float(fr["t"]) - (f + 1) / fps) < 1e-6
         assert fr["phi"].shape == cfg.res
+
+
+def test_step_without_particles_matches_oracle():
+    """An empty particle set, which the reference runs with its kernels
+    launched over zero threads: the grid is all air (phi = 0), gravity is
+    balanced against the walls by the pressure, and the library's steps match
+    the oracle's (CG iterations within one, pressure within 1e-4 of its
+    maximum after mean removal, the same CFL dt)."""
+    import os
+
+    from oracle import oracle as O
+
+    cfg = Config(res=(8,) * 3, dx=1 / 8, ppc=8, pcg_tol=1e-6, device=DEV)  # droplets on, as by default
+    e3, et = np.zeros((0, 3), np.float32), np.zeros(0, np.int32)
+    sim = Simulator(cfg)
+    sim.set_particles(e3, e3, et)
+    o = O.OracleSim(cfg, nthreads=os.cpu_count() or 1, stencil=cfg.stencil)
+    o.set_particles(e3, e3, et)
+    dt = sim.dt_from_cfl()
+    assert dt == pytest.approx(o.dt_from_cfl(), rel=1e-12)
+    for _ in range(2):
+        rg, ro = sim.step(dt), o.step(dt)
+        assert abs(rg["pcg_iter"] - ro["pcg_iter"]) <= 1 and rg["pcg_res"] < 1e-6 and rg["droplets"] == 0
+    assert np.abs(sim.phi_cell.numpy()).max() == 0.0
+    p, po = sim.pressure.numpy(), o.pressure
+    p, po = p - p.mean(), po - po.mean()
+    assert np.abs(p - po).max() <= 1e-4 * np.abs(po).max()
+    pos, vel = sim.read_particles()
+    assert pos.shape == (0, 3) and vel.shape == (0, 3)
+    assert sim.state_counts() == {"flip": 0, "droplet": 0, "dead": 0}
+    sim.set_particles(*scenes.dam_break(cfg))  # and particles can arrive later
+    assert sim.step(dt)["pcg_res"] < 1e-6
