@@ -161,6 +161,13 @@ def call(name: str, *args, ok=(PF_OK,)):
     return check(getattr(lib(), name)(*args), name, ok=ok)
 
 
+def sptr(t) -> int:
+    """Device address of a particle stream.  The simulator's streams are views
+    of the first n rows of at least one row of storage, so an empty stream
+    still has its storage's address (torch reports 0 for an empty tensor)."""
+    return t.untyped_storage().data_ptr() + t.storage_offset() * t.element_size()
+
+
 def ptr(t) -> int | None:
     """Raw device pointer of a tensor (or of a DeviceArray), None for None."""
     if t is None:

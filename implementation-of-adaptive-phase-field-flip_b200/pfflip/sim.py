@@ -381,13 +381,13 @@ class Simulator:
         """Counting sort of the particle streams by cell (new stage; the
         reference never reorders particles)."""
         n = self.n_particles
-        N.call("pf_sort_particles", C.byref(self._g), n, self._pos4.data_ptr(), self._vel4.data_ptr(),
-               self._pos4_alt.data_ptr(), self._vel4_alt.data_ptr(), self._keys.data_ptr(), self._perm.data_ptr(),
+        N.call("pf_sort_particles", C.byref(self._g), n, N.sptr(self._pos4), N.sptr(self._vel4),
+               N.sptr(self._pos4_alt), N.sptr(self._vel4_alt), N.sptr(self._keys), N.sptr(self._perm),
                self._cell_start.data_ptr(), self._sort_ws.data_ptr(), self._sort_ws.numel(), N.stream())
         self._pos4, self._pos4_alt = self._pos4_alt, self._pos4
         self._vel4, self._vel4_alt = self._vel4_alt, self._vel4
         if self.cfg.droplets:  # the droplet radius follows its particle
-            N.call("pf_permute_f32", n, self._perm.data_ptr(), self._drop_r.data_ptr(), self._drop_r_alt.data_ptr(),
+            N.call("pf_permute_f32", n, N.sptr(self._perm), N.sptr(self._drop_r), N.sptr(self._drop_r_alt),
                    N.stream())
             self._drop_r, self._drop_r_alt = self._drop_r_alt, self._drop_r
 
@@ -431,7 +431,7 @@ class Simulator:
         if self._vmax_valid:
             vmax = float(self._scal[2].item())
         else:
-            N.call("pf_particle_max_speed", self.n_particles, self._pos4.data_ptr(), self._vel4.data_ptr(),
+            N.call("pf_particle_max_speed", self.n_particles, N.sptr(self._pos4), N.sptr(self._vel4),
                    self._scal.data_ptr(), N.stream())
             vmax = float(self._scal[0].item())
         g = float(np.linalg.norm(cfg.gravity))
@@ -499,7 +499,7 @@ class Simulator:
             self._sort()
         if mark:
             mark("p2g")
-        N.call("pf_p2g", C.byref(self._g), self.n_particles, self._pos4.data_ptr(), self._vel4.data_ptr(),
+        N.call("pf_p2g", C.byref(self._g), self.n_particles, N.sptr(self._pos4), N.sptr(self._vel4),
                self._cell_start.data_ptr(), float(cfg.rho_l), float(cfg.rho_g), float(np.float32(cfg.r_p)),
                *(N.ptr(a) for a in self.mass), *(N.ptr(a) for a in self.mom), N.ptr(self.cell_mass),
                N.ptr(self.cell_wsum), N.stream())
@@ -566,8 +566,8 @@ class Simulator:
         if self._g2p_ws is None:
             nb = int(N.lib().pf_g2p_workspace_bytes(C.byref(self._g)))
             self._g2p_ws = torch.empty(nb, dtype=torch.uint8, device=self.dev)
-        N.call("pf_g2p_advect_packed", C.byref(self._g), self.n_particles, self._pos4.data_ptr(),
-               self._vel4.data_ptr(), *(N.ptr(a) for a in self.vel), *(N.ptr(a) for a in self.vel_star),
+        N.call("pf_g2p_advect_packed", C.byref(self._g), self.n_particles, N.sptr(self._pos4),
+               N.sptr(self._vel4), *(N.ptr(a) for a in self.vel), *(N.ptr(a) for a in self.vel_star),
                *(N.ptr(a) for a in self.vel_liq), N.ptr(self.solid) if self.has_solids else None,
                float(cfg.alpha_flip_liquid), float(cfg.alpha_flip_air), float(dt), lo, hi, int(do_g2p),
                int(do_advect), self._scal.data_ptr() + 8 if do_advect else None, self._g2p_ws.data_ptr(),
@@ -597,20 +597,20 @@ class Simulator:
         seed = (int(cfg.seed) + int(self.step_index)) & 0xFFFFFFFF
         g, n, st = C.byref(self._g), self.n_particles, N.stream()
         self._counters.zero_()
-        N.call("pf_droplet_classify", g, n, self._pos4.data_ptr(), self._vel4.data_ptr(), self._drop_r.data_ptr(),
+        N.call("pf_droplet_classify", g, n, N.sptr(self._pos4), N.sptr(self._vel4), N.sptr(self._drop_r),
                N.ptr(self.phi_cell), float(cfg.delta_phi), mu, sigma, float(r_min), float(r_max), seed,
                self._counters.data_ptr(), st)
         if cfg.spray_shear_threshold > 0.0:
             if self.shear is None:
                 self.shear = DeviceArray(torch.zeros(self.res, dtype=torch.float32, device=self.dev))
             N.call("pf_velocity_gradient", g, *(N.ptr(a) for a in self.vel), N.ptr(self.shear), st)
-            N.call("pf_spray_emit", g, n, self._pos4.data_ptr(), self._vel4.data_ptr(), self._drop_r.data_ptr(),
+            N.call("pf_spray_emit", g, n, N.sptr(self._pos4), N.sptr(self._vel4), N.sptr(self._drop_r),
                    N.ptr(self.phi_cell), N.ptr(self.shear), float(cfg.spray_shear_threshold),
                    float(cfg.spray_emission_rate), mu, sigma, float(r_min), float(r_max), seed,
                    self._counters.data_ptr(), st)
         lo, hi = self._bounds()
         grav = (C.c_float * 3)(*[float(x) for x in cfg.gravity])
-        N.call("pf_droplet_advance", g, n, self._pos4.data_ptr(), self._vel4.data_ptr(), self._drop_r.data_ptr(),
+        N.call("pf_droplet_advance", g, n, N.sptr(self._pos4), N.sptr(self._vel4), N.sptr(self._drop_r),
                *(N.ptr(a) for a in self.vel), float(dt), grav, float(cfg.rho_g), float(cfg.rho_l),
                float(cfg.droplet_drag_cd), float(cfg.evaporation_k * cfg.dx * cfg.dx), float(r_min), lo, hi,
                int(cfg.droplet_max_substeps), st)
@@ -627,7 +627,7 @@ class Simulator:
         if self.spray_density is None:
             self.spray_density = DeviceArray(torch.zeros(self.spray_res, dtype=torch.float16, device=self.dev))
         sx, sy, sz = self.spray_res
-        N.call("pf_spray_rasterize", self.n_particles, self._pos4.data_ptr(), self._drop_r.data_ptr(),
+        N.call("pf_spray_rasterize", self.n_particles, N.sptr(self._pos4), N.sptr(self._drop_r),
                N.ptr(self.spray_density), sx, sy, sz, float(self.dx_spray), N.stream())
         return self.spray_density
 
