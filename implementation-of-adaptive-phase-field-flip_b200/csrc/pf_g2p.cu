@@ -306,18 +306,24 @@ __device__ __forceinline__ int quad_row(const LeanFrame& f, int n1, int n2) {
   return (f.lo[0][Comp<C>::VI] * n1 + f.lo[1][Comp<C>::VJ]) * n2 + f.lo[2][Comp<C>::VK];
 }
 
-template <int C>
-__device__ __forceinline__ float sample_quad(const float4* __restrict__ q, const LeanFrame& f, int n1, int n2) {
-  const int row = quad_row<C>(f, n1, n2);
-  const float4 v0 = __ldg(q + row), v1 = __ldg(q + row + n1 * n2);
+// the two quads (lower and upper i-plane) of one component's field at the
+// taps of a frame, and the quad row they were read from
+struct QuadPair {
+  float4 lo, hi;
+  int row;
+};
+
+template <int C> __device__ __forceinline__ float lerp_pair(const QuadPair& q, const LeanFrame& f) {
   const float tj = f.t[1][Comp<C>::VJ], tk = f.t[2][Comp<C>::VK];
-  return lerpf(bilerp_q(v0, tj, tk), bilerp_q(v1, tj, tk), f.t[0][Comp<C>::VI]);
+  return lerpf(bilerp_q(q.lo, tj, tk), bilerp_q(q.hi, tj, tk), f.t[0][Comp<C>::VI]);
 }
 
-// G2P sample of component C: delta = I(u - u*) tap by tap, pic = I(u)
+// G2P sample of component C: delta = I(u - u*) tap by tap, pic = I(u); the u
+// quads stay in qp
 template <int C>
 __device__ __forceinline__ void sample_g2p_lean(const float4* __restrict__ qu, const float4* __restrict__ qs,
-                                                const LeanFrame& f, int n1, int n2, float& delta, float& pic) {
+                                                const LeanFrame& f, int n1, int n2, float& delta, float& pic,
+                                                QuadPair& qp) {
   const int row = quad_row<C>(f, n1, n2);
   const int up = n1 * n2;
   const float4 u0 = __ldg(qu + row), u1 = __ldg(qu + row + up);
@@ -327,16 +333,34 @@ __device__ __forceinline__ void sample_g2p_lean(const float4* __restrict__ qu, c
   const float4 d0 = make_float4(u0.x - s0.x, u0.y - s0.y, u0.z - s0.z, u0.w - s0.w);
   const float4 d1 = make_float4(u1.x - s1.x, u1.y - s1.y, u1.z - s1.z, u1.w - s1.w);
   delta = lerpf(bilerp_q(d0, tj, tk), bilerp_q(d1, tj, tk), ti);
+  qp.lo = u0;
+  qp.hi = u1;
+  qp.row = row;
+}
+
+// RK3 sample of component C at frame f through the quads of the previous
+// sample of the same field: a stage moves a particle a fraction of a cell, so
+// its taps mostly stay where they were and only the lanes whose taps moved
+// load.  The quads are the same values either way, so the sample is too.
+template <int C>
+__device__ __forceinline__ float sample_reuse(const float4* __restrict__ q, QuadPair& qp, const LeanFrame& f,
+                                              int n1, int n2) {
+  const int row = quad_row<C>(f, n1, n2);
+  if (row != qp.row) {
+    qp.lo = __ldg(q + row);
+    qp.hi = __ldg(q + row + n1 * n2);
+    qp.row = row;
+  }
+  return lerp_pair<C>(qp, f);
 }
 
 // RK3 sample of the velocity: liquid particles read the extrapolated field,
 // air the raw one
-__device__ __forceinline__ void sample_vel_lean(const G2PPackedArgs& a, bool liquid, const LeanFrame& f,
-                                                float out[3]) {
-  const int ny = a.ny, nz = a.nz;
-  out[0] = sample_quad<0>(liquid ? a.ql[0] : a.qu[0], f, ny, nz);
-  out[1] = sample_quad<1>(liquid ? a.ql[1] : a.qu[1], f, ny + 1, nz);
-  out[2] = sample_quad<2>(liquid ? a.ql[2] : a.qu[2], f, ny, nz + 1);
+__device__ __forceinline__ void sample_vel_reuse(const float4* const* fld, QuadPair qp[3], int ny, int nz,
+                                                 const LeanFrame& f, float out[3]) {
+  out[0] = sample_reuse<0>(fld[0], qp[0], f, ny, nz);
+  out[1] = sample_reuse<1>(fld[1], qp[1], f, ny + 1, nz);
+  out[2] = sample_reuse<2>(fld[2], qp[2], f, ny, nz + 1);
 }
 
 __global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(const __grid_constant__ G2PPackedArgs a) {
@@ -354,34 +378,40 @@ __global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(const __grid_const
     LeanFrame fx;
     if (flip && (a.do_g2p || a.do_advect)) lean_frame(x, a.inv_dx, nn, fx);
     float pic[3];  // I(u) at x: an air particle's first RK3 stage samples the same field there
+    QuadPair qp[3];  // per component, the quads of the last sample of the RK3 field
+#pragma unroll
+    for (int c = 0; c < 3; ++c) qp[c].row = -1;
     if (a.do_g2p && flip) {
       const float alpha = liquid ? a.a_liq : a.a_air;
       float delta[3];
-      sample_g2p_lean<0>(a.qu[0], a.qs[0], fx, a.ny, a.nz, delta[0], pic[0]);
-      sample_g2p_lean<1>(a.qu[1], a.qs[1], fx, a.ny + 1, a.nz, delta[1], pic[1]);
-      sample_g2p_lean<2>(a.qu[2], a.qs[2], fx, a.ny, a.nz + 1, delta[2], pic[2]);
+      sample_g2p_lean<0>(a.qu[0], a.qs[0], fx, a.ny, a.nz, delta[0], pic[0], qp[0]);
+      sample_g2p_lean<1>(a.qu[1], a.qs[1], fx, a.ny + 1, a.nz, delta[1], pic[1], qp[1]);
+      sample_g2p_lean<2>(a.qu[2], a.qs[2], fx, a.ny, a.nz + 1, delta[2], pic[2], qp[2]);
 #pragma unroll
       for (int c = 0; c < 3; ++c) v[c] = alpha * (v[c] + delta[c]) + (1.f - alpha) * pic[c];
     }
     if (a.do_advect) {
       if (flip) {
         float k1[3], k2[3], k3[3], y[3];
+        const float4* const* fld = liquid ? a.ql : a.qu;
         if (a.do_g2p && !liquid) {
 #pragma unroll
-          for (int c = 0; c < 3; ++c) k1[c] = pic[c];
+          for (int c = 0; c < 3; ++c) k1[c] = pic[c];  // qp holds the u quads at x
         } else {
-          sample_vel_lean(a, liquid, fx, k1);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) qp[c].row = -1;  // qp held u (liquid: the RK3 field is ul)
+          sample_vel_reuse(fld, qp, a.ny, a.nz, fx, k1);
         }
         const float h1 = 0.5f * a.dt, h2 = 0.75f * a.dt;
 #pragma unroll
         for (int c = 0; c < 3; ++c) y[c] = x[c] + h1 * k1[c];
         LeanFrame fy;
         lean_frame(y, a.inv_dx, nn, fy);
-        sample_vel_lean(a, liquid, fy, k2);
+        sample_vel_reuse(fld, qp, a.ny, a.nz, fy, k2);
 #pragma unroll
         for (int c = 0; c < 3; ++c) y[c] = x[c] + h2 * k2[c];
         lean_frame(y, a.inv_dx, nn, fy);
-        sample_vel_lean(a, liquid, fy, k3);
+        sample_vel_reuse(fld, qp, a.ny, a.nz, fy, k3);
         const float c1 = 2.0f / 9.0f, c2 = 3.0f / 9.0f, c3 = 4.0f / 9.0f;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
