@@ -31,7 +31,6 @@ import importlib.util
 import json
 import os
 import sys
-import textwrap
 import types
 
 import numpy as np

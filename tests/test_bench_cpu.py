@@ -3,7 +3,6 @@ the per-particle traffic the profiles supply, the peak it divides by, and the
 whole-job rate of N replicas."""
 
 import json
-import os
 
 import pytest
 

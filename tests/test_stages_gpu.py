@@ -19,7 +19,7 @@ import pytest
 import torch
 
 from oracle import oracle as O
-from pfflip import Config, Simulator, copy, scenes
+from pfflip import Config, Simulator, scenes
 from pfflip import _native as N
 
 pytestmark = pytest.mark.gpu
