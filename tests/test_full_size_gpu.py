@@ -5,8 +5,10 @@
   one oracle step fed the GPU's particle state at that step's input (so the
   summation-order drift of earlier steps does not compound), and the free run
   of 10 steps is compared with the free-running oracle.
-* The 128^3 dam break with 27 ppc (56,623,104 particles): one step, stage by
-  stage, the oracle fed the GPU state at each stage's input.
+* The 128^3 dam break with 27 ppc (56,623,104 particles) and the 256^3 / 8 ppc
+  Rayleigh-Taylor scene (134,217,728 particles): one step each, stage by
+  stage, the oracle fed the GPU state at each stage's input; and the
+  Rayleigh-Taylor scene at 32^3, each of 5 steps against one oracle step.
 * The standalone 128^3 solve (tanh slab + sphere, 1000:1, N(0,1) right-hand
   side) to 1e-6 in FP32 and with the FP16/BF16 hierarchy, against the binary64
   oracle solved to 1e-12.
@@ -88,9 +90,27 @@ def test_dam_break_128_27ppc_step_stages_match_oracle():
     """One step of the 56.6M-particle benchmark workload, stage by stage, after
     one warm step (so velocities are not zero)."""
     cfg = Config(res=(128, 128, 128), dx=1 / 128, ppc=27, seed=42, droplets=False, pcg_tol=1e-6)
+    pos, vel, pt = scenes.dam_break(cfg)
+    _step_stages_match_oracle(cfg, pos, vel, pt)
+
+
+def test_rayleigh_taylor_256_step_stages_match_oracle():
+    """One step of the 256^3 / 8 ppc Rayleigh-Taylor workload (134,217,728
+    particles, the displaced 16-mode lattice), stage by stage, after one warm
+    step from rest."""
+    import torch
+
+    from bench import rt_seed_device  # the benchmark's own seeding, displaced on the device
+
+    cfg = Config(res=(256, 256, 256), dx=1 / 256, ppc=8, seed=42, droplets=False, pcg_tol=1e-6)
+    pos, pt, _, _ = rt_seed_device(cfg, torch.device("cuda"))
+    _step_stages_match_oracle(cfg, pos, torch.zeros_like(pos), pt)
+
+
+def _step_stages_match_oracle(cfg, pos, vel, pt):
     dt = fixed_dt(cfg.dx)
     sim = Simulator(cfg)
-    sim.set_particles(*scenes.dam_break(cfg))
+    sim.set_particles(pos, vel, pt)
     sim.step(dt)
     o = oracle_from_sim(sim, cfg)
 
