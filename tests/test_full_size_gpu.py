@@ -180,9 +180,10 @@ def _step_stages_match_oracle(cfg, pos, vel, pt):
     sim._g2p_advect(dt, do_g2p=True, do_advect=True)
     o._g2p()
     o._advect(dt)
-    # 1e-5 dx, or two binary32 ulps of the domain size where that is coarser
-    # (at 256^3, 1e-5 dx = 3.9e-8 is below one ulp of a position near 1)
-    bar = max(1e-5 * cfg.dx, 2 * float(np.spacing(np.float32(max(cfg.domain_size)))))
+    # 1e-5 dx, or one binary32 ulp of the domain size (two ulps of a position
+    # just below it) where that is coarser: at 256^3, 1e-5 dx = 3.9e-8 is below
+    # one ulp of a position near 1
+    bar = max(1e-5 * cfg.dx, float(np.spacing(np.float32(max(cfg.domain_size)))))
     assert np.abs(sim.px.numpy() - o.px).max() < bar
     assert rel(sim.pv.numpy(), o.pv) < 1e-5
 
