@@ -19,11 +19,19 @@ reference package is then imported unchanged from its checkout and its
 every stage is saved.  The reference's host code (``sim.py``, ``poisson.py``
 outside the kernels) runs as ordinary Python, as it does under Warp.
 
+A further case drives the droplet stage (``pfflip/droplets.py`` through
+``Simulator._droplets``) and ``rasterize_spray`` on a state where every branch
+runs.  Warp's random stream (``rand_init``, ``randf``, ``randn``) is the one
+piece the stand-in replaces rather than restates: it draws on the stream the
+library documents for droplet radii and spray emission, so the rest of the
+droplet kernels, radii included, can be compared value for value.
+
 What this does not reproduce: the GPU's fused multiply-adds and the order of
 its atomics (both unspecified in the reference), so the fixtures pin the
 oracle to within the tolerances the stage tests use, not bit for bit.
 
-Output: ``ref_step.npz`` in this folder (tested by tests/test_oracle.py).
+Output: ``ref_step.npz`` in this folder (tested by tests/test_oracle.py and,
+for the droplet case, tests/test_droplets_gpu.py).
 """
 
 from __future__ import annotations
