@@ -438,6 +438,14 @@ __global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(const __grid_const
     a.pos[p] = P;
     a.vel[p] = V;
     if (flip) vmax = fmaxf(vmax, v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    // the records of the particle two iterations on into L2, so that its chain
+    // of dependent gathers starts from an L2 hit (a prefetch holds no
+    // register; issued here, where few values are live)
+    const long long q = p + 2 * (long long)gridDim.x * blockDim.x;
+    if (q < a.n) {
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(a.pos + q));
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(a.vel + q));
+    }
   }
   if (a.max_speed) {  // uniform: every thread of the grid takes this branch or none does
     __shared__ float sh[40];
