@@ -366,7 +366,15 @@ __device__ __forceinline__ void sample_vel_reuse(const float4* const* fld, QuadP
 __global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(const __grid_constant__ G2PPackedArgs a) {
   float vmax = 0.f;  // CFL speed^2 of this thread's FLIP particles (pfflip/kernels.py:552-564)
   const int nn[3] = {a.nx, a.ny, a.nz};
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
+  // each warp walks one contiguous chunk of the cell-sorted streams, 32
+  // particles at a time: its successive samples fall in neighbouring cells,
+  // whose quads are still in L1 (a grid-stride walk would jump to unrelated
+  // cells at every step)
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  const long long chunk = ((a.n + warps - 1) / warps + 31) & ~31LL;
+  const long long c0 = ((long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * chunk;
+  const long long c1 = c0 + chunk < a.n ? c0 + chunk : a.n;
+  for (long long p = c0 + (threadIdx.x & 31); p < c1; p += 32) {
     float4 P = a.pos[p];
     float4 V = a.vel[p];
     const int flags = __float_as_int(P.w);
@@ -441,8 +449,8 @@ __global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(const __grid_const
     // the records of the particle two iterations on into L2, so that its chain
     // of dependent gathers starts from an L2 hit (a prefetch holds no
     // register; issued here, where few values are live)
-    const long long q = p + 2 * (long long)gridDim.x * blockDim.x;
-    if (q < a.n) {
+    const long long q = p + 64;
+    if (q < c1) {
       asm volatile("prefetch.global.L2 [%0];" ::"l"(a.pos + q));
       asm volatile("prefetch.global.L2 [%0];" ::"l"(a.vel + q));
     }
