@@ -175,7 +175,9 @@ struct AdjG2PArgs {
 };
 
 __global__ void __launch_bounds__(128) k_adj_g2p_advect(AdjG2PArgs a) {
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
+  long long c0, c1;  // a contiguous chunk of the sorted streams per warp: gathers and scatters stay local
+  warp_chunk(a.n, c0, c1);
+  for (long long p = c0 + (threadIdx.x & 31); p < c1; p += 32) {
     const float4 P = a.pos[p], V = a.vel[p];
     const float4 GP = a.gpos_in[p], GV = a.gvel_in[p];
     const int flags = __float_as_int(P.w);
@@ -586,7 +588,9 @@ __device__ __forceinline__ void p2g_adjoint_grid(const AdjP2GArgs& a, int c, con
 }
 
 __global__ void __launch_bounds__(128) k_adj_p2g(const __grid_constant__ AdjP2GArgs a) {
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
+  long long c0, c1;  // a contiguous chunk of the sorted streams per warp: gathers stay local
+  warp_chunk(a.n, c0, c1);
+  for (long long p = c0 + (threadIdx.x & 31); p < c1; p += 32) {
     const float4 P = a.pos[p], V = a.vel[p];
     const int flags = __float_as_int(P.w);
     if (((flags >> PF_PSTATE_SHIFT) & 3) != 0) continue;

@@ -166,6 +166,17 @@ template <int NT> __device__ __forceinline__ float block_max(float v, float* sh 
 // counter.  Returns true in the last block (all threads), with *result valid
 // in every thread of that block.  The partials are read from L2 (__ldcg):
 // they were written by other blocks before their fenced ticket.
+// [c0, c1) of this warp's contiguous share of n items (a 1-D launch), in
+// multiples of 32: lane l takes items c0 + l, c0 + l + 32, ...  Over the
+// cell-sorted particle streams a warp's successive items lie in neighbouring
+// cells, so the grid values it gathers stay in L1 from one step to the next.
+__device__ __forceinline__ void warp_chunk(long long n, long long& c0, long long& c1) {
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  const long long chunk = ((n + warps - 1) / warps + 31) & ~31LL;
+  c0 = ((long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * chunk;
+  c1 = c0 + chunk < n ? c0 + chunk : n;
+}
+
 __device__ __forceinline__ unsigned lin_block() { return (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x; }
 __device__ __forceinline__ unsigned num_blocks() { return gridDim.x * gridDim.y * gridDim.z; }
 

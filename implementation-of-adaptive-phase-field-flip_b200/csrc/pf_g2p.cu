@@ -370,10 +370,8 @@ __global__ void __launch_bounds__(256, 3) k_g2p_advect_packed(const __grid_const
   // particles at a time: its successive samples fall in neighbouring cells,
   // whose quads are still in L1 (a grid-stride walk would jump to unrelated
   // cells at every step)
-  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-  const long long chunk = ((a.n + warps - 1) / warps + 31) & ~31LL;
-  const long long c0 = ((long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * chunk;
-  const long long c1 = c0 + chunk < a.n ? c0 + chunk : a.n;
+  long long c0, c1;
+  warp_chunk(a.n, c0, c1);
   for (long long p = c0 + (threadIdx.x & 31); p < c1; p += 32) {
     float4 P = a.pos[p];
     float4 V = a.vel[p];
