@@ -112,7 +112,9 @@ struct ClassifyArgs {
 // pfflip/droplets.py:67-106 classify_escaped
 __global__ void __launch_bounds__(256) k_droplet_classify(const __grid_constant__ ClassifyArgs a) {
   int emitted = 0, bubbles = 0, merged = 0;
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
+  long long c0, c1;  // a contiguous chunk of the sorted streams per warp: field samples stay in L1
+  warp_chunk(a.n, c0, c1);
+  for (long long p = c0 + (threadIdx.x & 31); p < c1; p += 32) {
     float4 P = a.pos[p];
     const int flags = __float_as_int(P.w);
     const int st = state_of(flags);
@@ -190,7 +192,9 @@ struct SprayArgs {
 // pfflip/droplets.py:112-150 emit_spray_in_shear
 __global__ void __launch_bounds__(256) k_spray_emit(const __grid_constant__ SprayArgs a) {
   int spray = 0;
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
+  long long c0, c1;  // a contiguous chunk of the sorted streams per warp: field samples stay in L1
+  warp_chunk(a.n, c0, c1);
+  for (long long p = c0 + (threadIdx.x & 31); p < c1; p += 32) {
     float4 P = a.pos[p];
     const int flags = __float_as_int(P.w);
     if (state_of(flags) != kStateFlip || (flags & PF_FLAG_LIQUID) == 0) continue;
@@ -224,7 +228,9 @@ struct AdvanceArgs {
 // dr/dt = -k/r by RK2; a droplet leaving the domain or shrinking below r_min
 // dies
 __global__ void __launch_bounds__(256) k_droplet_advance(AdvanceArgs a) {
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (long long)gridDim.x * blockDim.x) {
+  long long c0, c1;  // a contiguous chunk of the sorted streams per warp: field samples stay in L1
+  warp_chunk(a.n, c0, c1);
+  for (long long p = c0 + (threadIdx.x & 31); p < c1; p += 32) {
     float4 P = a.pos[p];
     const int flags = __float_as_int(P.w);
     if (state_of(flags) != kStateDroplet) continue;
@@ -277,7 +283,9 @@ __global__ void __launch_bounds__(256) k_droplet_advance(AdvanceArgs a) {
 __global__ void __launch_bounds__(256) k_spray_rasterize(long long n, const float4* __restrict__ pos,
                                                          const float* __restrict__ drop_r, __half* density, int sx,
                                                          int sy, int sz, float dxs) {
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+  long long c0, c1;  // a contiguous chunk per warp: its atomics land on neighbouring cells
+  warp_chunk(n, c0, c1);
+  for (long long p = c0 + (threadIdx.x & 31); p < c1; p += 32) {
     const float4 P = pos[p];
     if (state_of(__float_as_int(P.w)) != kStateDroplet) continue;
     const float r = drop_r[p];
