@@ -23,12 +23,17 @@
 namespace pf {
 
 // pass 1: key and arrival rank within the cell (ranks of one cell are
-// 0..count-1 in some order), counts into `counts`
+// 0..count-1 in some order), counts into `counts`.  Each warp walks one
+// contiguous chunk of the stream: on a stream already near cell order the
+// ranks of a cell then mostly arrive in index order, even where the cell
+// spans two batches of 32, so the order fix has less to do.
 __global__ void k_keys_rank(long long n, const float4* __restrict__ pos, float dx, int nx, int ny, int nz,
                             int2* __restrict__ key_rank, int* __restrict__ counts) {
-  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
-    const long long p = base + threadIdx.x;
-    const bool in = p < n;
+  long long c0, c1;
+  warp_chunk(n, c0, c1);
+  for (long long base = c0; base < c1; base += 32) {  // warp-uniform bound: every lane takes the ballot
+    const long long p = base + (threadIdx.x & 31);
+    const bool in = p < c1;
     const unsigned active = __ballot_sync(0xffffffffu, in);
     if (!in) continue;
     const float4 q = __ldg(pos + p);
