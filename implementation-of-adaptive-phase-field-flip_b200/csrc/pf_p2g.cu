@@ -208,18 +208,6 @@ template <int G> struct Box {
   }
 };
 
-// a particle record through the read-only path; the last pass over a row
-// (G == 2) marks its lines first to evict, since no pass reads them again,
-// so that they displace less of the rows other warps have yet to re-read
-template <int G> __device__ __forceinline__ float4 ld_particle(const float4* p) {
-  if (G != 2) return __ldg(p);
-  float4 v;
-  asm("ld.global.nc.L1::evict_first.v4.f32 {%0, %1, %2, %3}, [%4];"
-      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-      : "l"(p));
-  return v;
-}
-
 // one grid over the particles of cell (i, j, k) (range [s, e)), then the row flush
 template <int G>
 __device__ __forceinline__ void p2g_grid(const P2GArgs& a, float* acc, int i, int j, int k, int s, int e, int li,
@@ -233,20 +221,20 @@ __device__ __forceinline__ void p2g_grid(const P2GArgs& a, float* acc, int i, in
   const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
   float4 Pa = z4, Va = z4, Pb = z4, Vb = z4;
   if (s < e) {
-    Pa = ld_particle<G>(a.pos + s);
-    if (G < 3) Va = ld_particle<G>(a.vel + s);
+    Pa = __ldg(a.pos + s);
+    if (G < 3) Va = __ldg(a.vel + s);
   }
   if (s + 1 < e) {
-    Pb = ld_particle<G>(a.pos + s + 1);
-    if (G < 3) Vb = ld_particle<G>(a.vel + s + 1);
+    Pb = __ldg(a.pos + s + 1);
+    if (G < 3) Vb = __ldg(a.vel + s + 1);
   }
   for (int t = s; t < e; ++t) {
     const float4 P = Pa, V = Va;
     Pa = Pb;
     Va = Vb;
     if (t + 2 < e) {
-      Pb = ld_particle<G>(a.pos + t + 2);
-      if (G < 3) Vb = ld_particle<G>(a.vel + t + 2);
+      Pb = __ldg(a.pos + t + 2);
+      if (G < 3) Vb = __ldg(a.vel + t + 2);
     }
     const int flags = __float_as_int(P.w);
     if ((flags >> PF_PSTATE_SHIFT) & 3) continue;  // droplets / dead particles do not splat
