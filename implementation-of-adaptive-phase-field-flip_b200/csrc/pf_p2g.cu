@@ -29,7 +29,7 @@
 
 namespace pf {
 
-constexpr int PG_TI = 4, PG_TJ = 8, PG_TK = 32;
+constexpr int PG_TI = 2, PG_TJ = 8, PG_TK = 32;
 constexpr int PG_NT = 256;
 constexpr int PG_BI = PG_TI + 2, PG_BJ = PG_TJ + 2, PG_BK = PG_TK + 2;
 constexpr int PG_BOX = PG_BI * PG_BJ * PG_BK;  // nodes per accumulator box
