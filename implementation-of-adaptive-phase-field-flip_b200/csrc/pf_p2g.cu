@@ -306,6 +306,10 @@ extern "C" int pf_p2g(const pf_grid* g, int64_t n, const float* pos4, const floa
   static bool attr_set = false;
   if (!attr_set) {
     PF_CUDA_TRY(cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PG_SMEM));
+    // the smallest shared-memory carveout that holds two CTAs' accumulators,
+    // so that the rest of the SM's unified memory serves as L1 for the passes'
+    // re-reads (a hint: the driver rounds up to a carveout it supports)
+    PF_CUDA_TRY(cudaFuncSetAttribute(k_p2g, cudaFuncAttributePreferredSharedMemoryCarveout, 40));
     attr_set = true;
   }
   cudaStream_t s = S(stream);
