@@ -583,7 +583,9 @@ extern "C" int pf_g2p_advect_packed(const pf_grid* g, int64_t n, float* pos4, fl
   a.do_g2p = do_g2p;
   a.do_advect = do_advect;
   a.max_speed = max_speed;
-  k_g2p_advect_packed<<<grid_for(n, 256, kNumSMs * 16), 256, 0, s>>>(a);
+  // 64 CTAs per SM: warp chunks of ~750 particles at 128^3 / 27 ppc, long
+  // enough for the walk's L1 reuse, short enough that the chunks balance
+  k_g2p_advect_packed<<<grid_for(n, 256, kNumSMs * 64), 256, 0, s>>>(a);
   PF_LAUNCHED();
   return PF_OK;
 }
